@@ -1,0 +1,147 @@
+/*
+ * via_gpu.h — C ABI of the B200 VIA server answer path.
+ *
+ * This library is a drop-in for the reference (roynalnaruto/via-rs) server API
+ * `via_server::Server` (crates/via-server/src/answer.rs:423-603):
+ *
+ *   Server::setup(ServerConfig, &[RRec], p_mod)  -> via_server_setup
+ *   Server::answer(&CompressedQuery)             -> via_server_answer
+ *   Server::answer_batch::<T>(&BatchedQuery)     -> via_server_answer_batch
+ *   drop(Server)                                 -> via_server_destroy
+ *
+ * plus the free kernel boundaries the reference names for a GPU build
+ * (`first_dim`, crates/via-server/src/first_dim.rs:94; the eval-form gadget
+ * product, crates/via-primitives/src/encryption/rlev.rs:259) as device-pointer
+ * entry points for parity tests and micro-benchmarks.
+ *
+ * Conventions
+ *  - Plain C99: opaque handles, caller-owned buffers of little-endian uint64_t
+ *    residues, an int status. No CUDA or torch types cross the boundary; a
+ *    stream is passed as `void*` (a cudaStream_t, or NULL for the default).
+ *  - All ciphertext buffers use the reference's in-memory layout:
+ *      poly   : nl limb arrays of n residues, limb 0 first
+ *               (PolyRns, crates/via-primitives/src/algebra/ring/rns_element.rs:44-54);
+ *               nl = 2 at q1 when q1 is a two-prime RNS basis, else 1.
+ *      RLWE   : mask poly, then body poly.
+ *      RLev   : L RLWE samples, samples[0] paired with the largest gadget entry
+ *               (crates/via-primitives/src/encryption/types.rs:148-251).
+ *      LWE    : MLWECiphertext<n1, 1> (crates/via-primitives/src/encryption/mlwe.rs:27-39)
+ *               stored as its mask polynomial (nl*n1, coefficient i = masks[i])
+ *               followed by the body (nl residues).
+ *      query  : the CompressedQuery's LWEs in order (DMux bits MSB-first,
+ *               CMux bits LSB-first, CRot bits LSB-first, L_QUERY levels each).
+ *      answer : ModSwitchedCiphertext<n2> = mask (n2 residues mod q3) then
+ *               body (n2 residues mod q4).
+ *  - Status codes are the reference's ViaError discriminants + 1
+ *    (crates/via-protocol/src/error.rs:20-64), then device-side codes.
+ */
+#ifndef VIA_GPU_H
+#define VIA_GPU_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum via_status {
+  VIA_OK = 0,
+  VIA_ERR_SETUP_NOT_COMPLETE = 1,      /* ViaError::SetupNotComplete */
+  VIA_ERR_INDEX_OUT_OF_RANGE = 2,      /* ViaError::IndexOutOfRange */
+  VIA_ERR_QUERY_LENGTH_MISMATCH = 3,   /* ViaError::QueryLengthMismatch */
+  VIA_ERR_BUFFER_TOO_SHORT = 4,        /* ViaError::BufferTooShort */
+  VIA_ERR_UNKNOWN_FORMAT_TAG = 5,      /* ViaError::UnknownFormatTag */
+  VIA_ERR_INVALID_PRG_SEED = 6,        /* ViaError::InvalidPrgSeed */
+  VIA_ERR_DIM_MISMATCH = 7,            /* ViaError::DimMismatch */
+  VIA_ERR_INVALID_ARGUMENT = 100,      /* null handle/pointer, unsupported parameter */
+  VIA_ERR_OUT_OF_MEMORY = 101,         /* device allocation or HBM budget exhausted */
+  VIA_ERR_CUDA = 102,                  /* a CUDA runtime call failed */
+  VIA_ERR_TIMEOUT = 103,               /* a bounded wait expired */
+  VIA_ERR_BUSY = 104                   /* serving queue full; retry later */
+} via_status;
+
+/*
+ * Runtime mirror of the reference's const-generic preset + PIRParams
+ * (crates/via-protocol/src/params.rs:59-125, presets.rs:204-258) and the
+ * server's DB dimensions (PublicParams.num_rows/num_cols) and record degree
+ * N_REC (answer.rs:423-434).
+ */
+typedef struct via_params {
+  uint32_t n1;        /* large ring degree (power of two) */
+  uint32_t n2;        /* small ring degree, n1 = d * n2 */
+  uint32_t n_rec;     /* record degree: n2 for VIA-C, n3 for VIA-B */
+  uint32_t reserved0;
+  uint64_t num_rows;  /* I (power of two) */
+  uint64_t num_cols;  /* J (power of two) */
+  uint64_t q1_0;      /* q1 = q1_0 * q1_1 (two-prime RNS) ... */
+  uint64_t q1_1;      /* ... or q1 = q1_0 when q1_1 == 0 */
+  uint64_t q2, q3, q4, p;
+  uint64_t b_dmux;    /* gadget_base_1 (DMux @ q1) */
+  uint64_t b_cmux;    /* gadget_base_2 (CMux / CRot @ q2) */
+  uint64_t ck_base;   /* cascade + conversion-key gadget base */
+  uint64_t b_rsk;     /* ring-switch gadget base */
+  uint32_t l_query;   /* L_QUERY: LWEs per query bit = RGSW gadget depth */
+  uint32_t l_ck;      /* L_CK: cascade / conversion-key depth */
+  uint32_t l_rsk;     /* L_RSK: ring-switch key depth */
+  uint32_t reserved1;
+} via_params;
+
+/* Record encodings accepted by via_server_setup. */
+typedef enum via_record_format {
+  VIA_RECORDS_U64 = 0,    /* n_rec uint64_t coefficients per record (reference RRec layout) */
+  VIA_RECORDS_NIBBLE = 1  /* n_rec/2 bytes per record, two 4-bit coefficients per byte,
+                             low nibble first (requires p <= 16) */
+} via_record_format;
+
+/* The client's public keys (reference PublicParams, crates/via-protocol/src/wire/keys.rs:29-108). */
+typedef struct via_public_keys {
+  const uint64_t* cascade_key; /* LWE->RLWE cascade key: for k = 1..log2 n1, RANK_IN = n1>>(k-1)
+                                  RLevs of L_CK samples at degree 2^k over q1 (prim/conversion/cascade.rs) */
+  const uint64_t* conv_key;    /* RLev_{S1}(S1^2): L_CK samples at (q1, n1) */
+  const uint64_t* rsk;         /* ring-switch key: d RLevs of L_RSK samples at (q3, n2) */
+} via_public_keys;
+
+typedef struct via_server via_server;
+
+/* Buffer sizes in uint64_t units. */
+uint64_t via_lwe_len(const via_params* p);
+uint64_t via_query_len(const via_params* p);          /* number of LWEs in a query */
+uint64_t via_cascade_key_len(const via_params* p);
+uint64_t via_conv_key_len(const via_params* p);
+uint64_t via_rsk_len(const via_params* p);
+
+/*
+ * Server::setup (answer.rs:486-528): encodes the records into the I x J cell
+ * matrix (setup_db.rs:39-75), lifts them to q2 and forward-transforms them on
+ * the device once (prepared_db.rs:57-85), and uploads the eval-form public keys
+ * (prepared_keys.rs:69-79). Fewer records than capacity are zero-padded; more
+ * is VIA_ERR_DIM_MISMATCH. Uses device 0 unless via_set_device was called.
+ */
+via_status via_server_setup(const via_params* params, const via_public_keys* keys, const void* records,
+                            uint64_t n_records, via_record_format format, via_server** out);
+
+/*
+ * Server::answer (answer.rs:534-554): steps 1-7 on the device for one query.
+ * out_mask: n2 residues mod q3; out_body: n2 residues mod q4. Host buffers.
+ */
+via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
+                             uint64_t* out_body);
+
+void via_server_destroy(via_server* s);
+
+/* Message for the last failing call on this thread ("" if none). */
+const char* via_last_error(void);
+
+/*
+ * FirstDim (first_dim.rs:94-184) on device buffers: `switched` holds I RLWEs at
+ * (q2, n1) in coefficient form; `out` receives the J column RLWEs. The server's
+ * prepared database is the other operand.
+ */
+via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* out, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* VIA_GPU_H */

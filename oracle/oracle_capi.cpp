@@ -1,0 +1,258 @@
+// C ABI of the CPU oracle — TEST INFRASTRUCTURE ONLY (tests/, smoke(), the
+// bench's CPU-baseline leg). Buffers use the wire layouts of include/via_gpu.h.
+#include <cstring>
+#include <map>
+#include <memory>
+
+#include "../include/via_gpu.h"
+#include "via_oracle.hpp"
+
+namespace vo {
+std::map<std::string, std::vector<u64>> run_kat(const std::string& layer, const std::string& scenario);
+}
+
+using namespace vo;
+
+static thread_local std::string g_err;
+
+static Params to_params(const via_params* p) {
+  Params r;
+  r.n1 = (int)p->n1;
+  r.n2 = (int)p->n2;
+  r.n_rec = (int)p->n_rec;
+  r.num_rows = p->num_rows;
+  r.num_cols = p->num_cols;
+  r.q1_0 = p->q1_0;
+  r.q1_1 = p->q1_1;
+  r.q2 = p->q2;
+  r.q3 = p->q3;
+  r.q4 = p->q4;
+  r.p = p->p;
+  r.b_dmux = p->b_dmux;
+  r.b_cmux = p->b_cmux;
+  r.ck_base = p->ck_base;
+  r.b_rsk = p->b_rsk;
+  r.l_query = (int)p->l_query;
+  r.l_ck = (int)p->l_ck;
+  r.l_rsk = (int)p->l_rsk;
+  return r;
+}
+
+template <class F>
+static int guarded(F f) {
+  try {
+    f();
+    return 0;
+  } catch (const OracleError& e) {
+    g_err = e.what();
+    return e.code;
+  } catch (const std::exception& e) {
+    g_err = e.what();
+    return ERR_INVALID;
+  }
+}
+
+// ---- flat (de)serialisation in the include/via_gpu.h layouts -------------
+static void put_poly(u64*& dst, const Poly& a) {
+  std::memcpy(dst, a.data(), a.size() * 8);
+  dst += a.size();
+}
+static Poly get_poly(const u64*& src, size_t n) {
+  Poly a(src, src + n);
+  src += n;
+  return a;
+}
+static void put_rlev(u64*& dst, const Rlev& r) {
+  for (auto& s : r) {
+    put_poly(dst, s.mask);
+    put_poly(dst, s.body);
+  }
+}
+static Rlev get_rlev(const u64*& src, const Ring& R, int L) {
+  Rlev r;
+  for (int l = 0; l < L; ++l) {
+    Rlwe s;
+    s.mask = get_poly(src, R.size());
+    s.body = get_poly(src, R.size());
+    r.push_back(s);
+  }
+  return r;
+}
+static CascadeKey get_cascade(const u64*& src, const Ring& R, int L) {
+  CascadeKey K;
+  K.n = R.n;
+  K.L = L;
+  for (int nout = 2; nout <= R.n; nout <<= 1) {
+    int rank_in = R.n / (nout / 2);
+    Ring Ro = R.with_n(nout);
+    std::vector<Rlev> step;
+    for (int i = 0; i < rank_in; ++i) step.push_back(get_rlev(src, Ro, L));
+    K.steps.push_back(step);
+  }
+  return K;
+}
+static std::vector<Lwe> get_query(const u64* src, const Ring& R, size_t n_lwe) {
+  std::vector<Lwe> q;
+  for (size_t i = 0; i < n_lwe; ++i) {
+    Lwe l;
+    l.mask_poly = get_poly(src, R.size());
+    l.body = get_poly(src, R.nl);
+    q.push_back(l);
+  }
+  return q;
+}
+
+struct OracleServer {
+  Params prm;
+  PreparedKeys keys;
+  PreparedDb db;
+};
+
+extern "C" {
+
+const char* vo_last_error(void) { return g_err.c_str(); }
+
+void vo_shake256(const uint8_t* in, size_t inlen, uint8_t* out, size_t outlen) { shake256(in, inlen, out, outlen); }
+
+// Runs one replayed reference KAT and copies the named output. Returns the
+// number of values (or -code on error; -1 if the name is unknown).
+long vo_kat(const char* layer, const char* scenario, const char* name, uint64_t* out, size_t cap) {
+  long n = -1;
+  int rc = guarded([&] {
+    auto o = run_kat(layer, scenario);
+    auto it = o.find(name);
+    if (it == o.end()) return;
+    n = (long)it->second.size();
+    std::memcpy(out, it->second.data(), std::min((size_t)n, cap) * 8);
+  });
+  return rc ? -rc : n;
+}
+
+// Client::setup (cli/client.rs:89-180) with ternary keys and errors; writes the
+// public keys in wire layout. Returns an opaque client or NULL.
+void* vo_client_setup(const via_params* p, const uint8_t* seed, size_t seedlen, uint64_t* cascade, uint64_t* conv,
+                      uint64_t* rsk) {
+  Client* out = nullptr;
+  guarded([&] {
+    Params prm = to_params(p);
+    Prg prg(seed, seedlen);
+    PublicKeys pk;
+    Dist T = Dist::ternary();
+    auto c = std::make_unique<Client>(client_setup(prm, T, T, T, prg, pk));
+    u64* d = cascade;
+    for (auto& st : pk.cascade.steps)
+      for (auto& rl : st) put_rlev(d, rl);
+    d = conv;
+    put_rlev(d, pk.conv_key);
+    d = rsk;
+    for (auto& r : pk.rsk) put_rlev(d, r);
+    out = c.release();
+  });
+  return out;
+}
+
+// Client::query / batch_query (cli/client.rs:183-220): `d` is n1 / n_rec.
+int vo_client_query(void* c, uint64_t index, uint32_t d, const uint8_t* seed, size_t seedlen, uint64_t* out) {
+  return guarded([&] {
+    Client* cl = (Client*)c;
+    Prg prg(seed, seedlen);
+    std::vector<Lwe> q = client_query(*cl, index, (int)d, prg);
+    u64* dst = out;
+    for (auto& l : q) {
+      put_poly(dst, l.mask_poly);
+      put_poly(dst, l.body);
+    }
+  });
+}
+
+// Client::recover (cli/client.rs:222-237): n2 plaintext coefficients.
+int vo_client_recover(void* c, const uint64_t* mask, const uint64_t* body, uint64_t* out) {
+  return guarded([&] {
+    Client* cl = (Client*)c;
+    int n2 = cl->prm.n2;
+    Poly m(mask, mask + n2), b(body, body + n2);
+    std::vector<u64> r = client_recover(*cl, m, b);
+    std::memcpy(out, r.data(), r.size() * 8);
+  });
+}
+
+void vo_client_free(void* c) { delete (Client*)c; }
+
+// Server::setup (srv/answer.rs:486-528). Records: n_rec u64 coefficients each.
+void* vo_server_setup(const via_params* p, const uint64_t* cascade, const uint64_t* conv, const uint64_t* rsk,
+                      const uint64_t* records, size_t n_records, int threads) {
+  OracleServer* out = nullptr;
+  guarded([&] {
+    auto s = std::make_unique<OracleServer>();
+    s->prm = to_params(p);
+    const Params& prm = s->prm;
+    Ring R1 = prm.r1(), R3 = prm.r3();
+    PublicKeys pk;
+    const u64* src = cascade;
+    pk.cascade = get_cascade(src, R1, prm.l_ck);
+    src = conv;
+    pk.conv_key = get_rlev(src, R1, prm.l_ck);
+    src = rsk;
+    for (int j = 0; j < prm.d(); ++j) pk.rsk.push_back(get_rlev(src, R3, prm.l_rsk));
+    s->keys = prepare_keys(prm, pk);
+    s->db = setup_db(prm, records, n_records, threads);
+    out = s.release();
+  });
+  return out;
+}
+
+int vo_server_answer(void* sv, const uint64_t* query, size_t n_lwe, uint64_t* mask, uint64_t* body, int threads) {
+  return guarded([&] {
+    OracleServer* s = (OracleServer*)sv;
+    Ring R1 = s->prm.r1();
+    std::vector<Lwe> q = get_query(query, R1, n_lwe);
+    Poly m, b;
+    answer(s->prm, q, s->keys, s->db, threads, m, b);
+    std::memcpy(mask, m.data(), m.size() * 8);
+    std::memcpy(body, b.data(), b.size() * 8);
+  });
+}
+
+// Steps 1..6 only (srv/answer.rs:83-228): the CRot output RLWE at (q2, n1).
+int vo_server_answer_through_crot(void* sv, const uint64_t* query, size_t n_lwe, uint64_t* out, int threads) {
+  return guarded([&] {
+    OracleServer* s = (OracleServer*)sv;
+    std::vector<Lwe> q = get_query(query, s->prm.r1(), n_lwe);
+    Rlwe r = answer_through_crot(s->prm, q, s->keys, s->db, threads);
+    u64* d = out;
+    put_poly(d, r.mask);
+    put_poly(d, r.body);
+  });
+}
+
+// FirstDim (srv/first_dim.rs:94-184): I RLWEs at (q2, n1) -> J RLWEs.
+int vo_server_first_dim(void* sv, const uint64_t* switched, uint64_t* out, int threads) {
+  return guarded([&] {
+    OracleServer* s = (OracleServer*)sv;
+    int n = s->prm.n1;
+    std::vector<Rlwe> in;
+    const u64* src = switched;
+    for (u64 i = 0; i < s->prm.num_rows; ++i) {
+      Rlwe c;
+      c.mask = get_poly(src, n);
+      c.body = get_poly(src, n);
+      in.push_back(c);
+    }
+    std::vector<Rlwe> r = first_dim(s->prm, in, s->db, threads);
+    u64* d = out;
+    for (auto& c : r) {
+      put_poly(d, c.mask);
+      put_poly(d, c.body);
+    }
+  });
+}
+
+// Seconds spent in steps 1..7 by the last vo_server_answer on this thread.
+void vo_stage_times(double* out7) {
+  const StageTimes& t = last_stage_times();
+  for (int i = 0; i < 7; ++i) out7[i] = t.t[i];
+}
+
+void vo_server_free(void* s) { delete (OracleServer*)s; }
+
+}  // extern "C"

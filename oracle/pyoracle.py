@@ -1,0 +1,168 @@
+"""ctypes binding of the CPU oracle — TEST INFRASTRUCTURE ONLY.
+
+Loaded by tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg, as
+the checker. The product path (via_rs_b200) never imports this module.
+"""
+import ctypes
+import os
+import pathlib
+
+import numpy as np
+
+from via_rs_b200.params import Params
+
+_HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = _HERE / "_build" / "libvia_oracle.so"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+
+
+def build() -> None:
+    """Compile the oracle with its Makefile (g++)."""
+    import subprocess
+
+    subprocess.run(["make", "-s", "-C", str(_HERE)], check=True)
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        L = ctypes.CDLL(str(LIB_PATH))
+        L.vo_last_error.restype = ctypes.c_char_p
+        L.vo_kat.restype = ctypes.c_long
+        L.vo_kat.argtypes = [ctypes.c_char_p, ctypes.c_char_p, ctypes.c_char_p, _u64p, ctypes.c_size_t]
+        L.vo_client_setup.restype = ctypes.c_void_p
+        L.vo_client_setup.argtypes = [ctypes.c_void_p, ctypes.c_char_p, ctypes.c_size_t, _u64p, _u64p, _u64p]
+        L.vo_client_query.argtypes = [ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint32, ctypes.c_char_p,
+                                      ctypes.c_size_t, _u64p]
+        L.vo_client_recover.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p]
+        L.vo_client_free.argtypes = [ctypes.c_void_p]
+        L.vo_server_setup.restype = ctypes.c_void_p
+        L.vo_server_setup.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p, _u64p, ctypes.c_size_t, ctypes.c_int]
+        L.vo_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, _u64p, ctypes.c_int]
+        L.vo_server_answer_through_crot.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
+        L.vo_server_first_dim.argtypes = [ctypes.c_void_p, _u64p, _u64p, ctypes.c_int]
+        L.vo_server_free.argtypes = [ctypes.c_void_p]
+        L.vo_stage_times.argtypes = [ctypes.POINTER(ctypes.c_double)]
+        L.vo_shake256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
+        _lib = L
+    return _lib
+
+
+def _ptr(a: np.ndarray):
+    assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
+    return a.ctypes.data_as(_u64p)
+
+
+class OracleError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"oracle error {code}: {msg}")
+        self.code = code
+
+
+def _check(rc: int) -> None:
+    if rc != 0:
+        raise OracleError(rc, lib().vo_last_error().decode())
+
+
+def shake256(data: bytes, n: int) -> bytes:
+    out = ctypes.create_string_buffer(n)
+    lib().vo_shake256(data, len(data), out, n)
+    return out.raw
+
+
+def kat(layer: str, scenario: str, name: str, cap: int = 4096) -> np.ndarray:
+    out = np.zeros(cap, dtype=np.uint64)
+    n = lib().vo_kat(layer.encode(), scenario.encode(), name.encode(), _ptr(out), cap)
+    if n < 0:
+        raise OracleError(-n, f"{layer}/{scenario}/{name}: " + lib().vo_last_error().decode())
+    return out[:n].copy()
+
+
+class Client:
+    """Client::setup / query / recover (crates/via-client/src/client.rs)."""
+
+    def __init__(self, prm: Params, seed: bytes):
+        self.prm = prm
+        self.cascade_key = np.zeros(prm.cascade_key_len, dtype=np.uint64)
+        self.conv_key = np.zeros(prm.conv_key_len, dtype=np.uint64)
+        self.rsk = np.zeros(prm.rsk_len, dtype=np.uint64)
+        self._cp = prm.to_c()
+        h = lib().vo_client_setup(ctypes.byref(self._cp), seed, len(seed), _ptr(self.cascade_key),
+                                  _ptr(self.conv_key), _ptr(self.rsk))
+        if not h:
+            raise OracleError(-1, lib().vo_last_error().decode())
+        self._h = h
+
+    def query(self, index: int, seed: bytes, d: int | None = None) -> np.ndarray:
+        prm = self.prm
+        d = prm.n1 // prm.n_rec if d is None else d
+        n = (prm.num_dmux + prm.num_cmux + (d.bit_length() - 1 if d > 1 else 0)) * prm.l_query
+        out = np.zeros(n * prm.lwe_len, dtype=np.uint64)
+        _check(lib().vo_client_query(self._h, index, d, seed, len(seed), _ptr(out)))
+        return out
+
+    def recover(self, mask: np.ndarray, body: np.ndarray) -> np.ndarray:
+        out = np.zeros(self.prm.n2, dtype=np.uint64)
+        _check(lib().vo_client_recover(self._h, _ptr(np.ascontiguousarray(mask, dtype=np.uint64)),
+                                       _ptr(np.ascontiguousarray(body, dtype=np.uint64)), _ptr(out)))
+        return out
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().vo_client_free(self._h)
+            self._h = None
+
+
+class Server:
+    """Server::setup / answer on the CPU (crates/via-server/src/answer.rs)."""
+
+    def __init__(self, prm: Params, cascade_key, conv_key, rsk, records: np.ndarray, threads: int = 0):
+        self.prm = prm
+        self.threads = threads or os.cpu_count() or 1
+        self._cp = prm.to_c()
+        rec = np.ascontiguousarray(records, dtype=np.uint64)
+        n_rec = rec.size // prm.n_rec
+        h = lib().vo_server_setup(ctypes.byref(self._cp), _ptr(cascade_key), _ptr(conv_key), _ptr(rsk),
+                                  _ptr(rec), n_rec, self.threads)
+        if not h:
+            raise OracleError(-1, lib().vo_last_error().decode())
+        self._h = h
+
+    def answer(self, query: np.ndarray):
+        prm = self.prm
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        mask = np.zeros(prm.n2, dtype=np.uint64)
+        body = np.zeros(prm.n2, dtype=np.uint64)
+        _check(lib().vo_server_answer(self._h, _ptr(q), q.size // prm.lwe_len, _ptr(mask), _ptr(body),
+                                      self.threads))
+        return mask, body
+
+    def answer_through_crot(self, query: np.ndarray) -> np.ndarray:
+        prm = self.prm
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        out = np.zeros(2 * prm.n1, dtype=np.uint64)
+        _check(lib().vo_server_answer_through_crot(self._h, _ptr(q), q.size // prm.lwe_len, _ptr(out),
+                                                   self.threads))
+        return out
+
+    def first_dim(self, switched: np.ndarray) -> np.ndarray:
+        prm = self.prm
+        out = np.zeros(prm.num_cols * 2 * prm.n1, dtype=np.uint64)
+        _check(lib().vo_server_first_dim(self._h, _ptr(np.ascontiguousarray(switched, dtype=np.uint64)),
+                                         _ptr(out), self.threads))
+        return out
+
+    @staticmethod
+    def stage_times():
+        t = (ctypes.c_double * 7)()
+        lib().vo_stage_times(t)
+        return list(t)
+
+    def __del__(self):
+        if getattr(self, "_h", None):
+            lib().vo_server_free(self._h)
+            self._h = None
