@@ -1,0 +1,333 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 VIA server answer path.
+
+Workload (one step = one answer of one query): the paper VIA-C preset
+(n1=2048, n2=512, q1 two 37/38-bit primes, q2 34-bit) over a 1 GiB database of
+4-bit records laid out I=2^8 x J=2^12 (the reference's docs/params.html Table 4
+dimensions for 1 GiB). The prepared database is 16 GiB in HBM (one u64 residue
+per eval slot), far larger than L2, so every step streams it from DRAM.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Prints one JSON line (rank 0). `value` is whole-job answers/s with the query
+already resident on the device; `e2e` is the same through the host-buffer C ABI
+call via_server_answer (query upload and answer download inside the timed
+region). With N > 1 (torchrun) every rank answers on its own full replica
+("replicas only": the answer path does not shard), timed as the max over ranks.
+"""
+import argparse
+import ctypes
+import json
+import os
+import pathlib
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = pathlib.Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "answers/s and DB GB/s scanned, batched vs plain, 1 GiB DB; p50/p99 answer ms"
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_first_dim_ntt launch,
+# scaled to the 1 GiB workload (see profiles/first_dim_scan.md); None until captured.
+SCAN_TRAFFIC_BYTES = None
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--rows", type=int, default=256)
+    ap.add_argument("--cols", type=int, default=4096)
+    ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU oracle leg (for profiling)")
+    ap.add_argument("--scan-launches", type=int, default=10)
+    return ap.parse_args()
+
+
+def load_peaks():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---------------------------------------------------------------------------
+# Synthetic inputs (seeded). Key and query residues are uniform: the answer's
+# cost does not depend on their values; correctness is covered by the tests.
+# ---------------------------------------------------------------------------
+def make_inputs(prm, seed):
+    from via_rs_b200.server import PublicKeys
+
+    rng = np.random.default_rng(seed)
+    qmin = min(prm.q1)
+    records = rng.integers(0, 256, size=prm.capacity * prm.n_rec // 2, dtype=np.uint8)
+    keys = PublicKeys(rng.integers(0, qmin, size=prm.cascade_key_len, dtype=np.uint64),
+                      rng.integers(0, qmin, size=prm.conv_key_len, dtype=np.uint64),
+                      rng.integers(0, prm.q3, size=prm.rsk_len, dtype=np.uint64))
+    query = rng.integers(0, qmin, size=prm.n_lwe * prm.lwe_len, dtype=np.uint64)
+    return records, keys, query
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+              "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+              "clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index):
+        self.index = index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [x.strip() for x in ln.split(",")]
+            if len(parts) < 7:
+                continue
+            try:
+                sm.append(float(parts[0]))
+                smax.append(float(parts[1]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[3:7]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# CPU baseline: the oracle (a restatement of the reference's Rust server) on a
+# bounded sample, extrapolated to the full workload per pipeline stage.
+# ---------------------------------------------------------------------------
+def cpu_answer_sample(prm, sample_cols=32, seed=7):
+    from oracle import pyoracle
+
+    sprm = prm.with_dims(prm.num_rows, sample_cols)
+    records, keys, _ = make_inputs(sprm, seed)
+    rec = np.empty(records.size * 2, dtype=np.uint64)
+    rec[0::2] = records & 15
+    rec[1::2] = records >> 4
+    threads = os.cpu_count() or 1
+    srv = pyoracle.Server(sprm, keys.cascade_key, keys.conv_key, keys.rsk, rec, threads)
+    q = np.random.default_rng(seed).integers(0, min(prm.q1), size=sprm.n_lwe * sprm.lwe_len, dtype=np.uint64)
+    t0 = time.perf_counter()
+    srv.answer(q)
+    wall = time.perf_counter() - t0
+    st = srv.stage_times()  # decomp, dmux, modswitch, firstdim, cmux, crot, respcomp
+    scale_cols = prm.num_cols / sample_cols
+    t = (st[0] * prm.n_lwe / sprm.n_lwe + st[1] + st[2] + st[3] * scale_cols
+         + st[4] * (prm.num_cols - 1) / (sample_cols - 1) + st[5] + st[6])
+    sample = (f"oracle answer at I={prm.num_rows}, J={sample_cols} ({wall:.2f} s on {threads} threads), "
+              f"stages extrapolated to J={prm.num_cols} and {prm.n_lwe} query LWEs")
+    return t, threads, sample
+
+
+def reference_arm(args, prm):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    times = []
+    threads, sample = 0, ""
+    for i in range(args.warmup + args.steps):
+        t, threads, sample = cpu_answer_sample(prm, seed=7 + i)
+        if i >= args.warmup:
+            times.append(t)
+    t_step = sum(times) / len(times)
+    value = 1.0 / t_step
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": "answers/s", "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": t_step * 1e3, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
+        "config": config_dict(prm),
+        "cpu_baseline": {"value": value, "unit": "answers/s", "cores": threads, "kind": "port",
+                         "sample": sample + "; Rust toolchain unavailable, so the C++ oracle restatement is timed"},
+        "e2e": {"value": value, "unit": "answers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def config_dict(prm):
+    return {"workload": f"paper VIA-C answer, 1 GiB DB (I={prm.num_rows}, J={prm.num_cols}, n1={prm.n1}), "
+                        "one query per step",
+            "preset": "paper (q1=137438822401*274810798081, q2=17175674881, q3=8380417, q4=4096, p=16)",
+            "db_raw_bytes": prm.capacity * prm.n_rec // 2, "db_prepared_bytes": prm.num_rows * prm.num_cols * prm.n1 * 8,
+            "l2": "inputs larger than L2: the 16 GiB prepared DB is streamed every step"}
+
+
+# ---------------------------------------------------------------------------
+# GPU arm.
+# ---------------------------------------------------------------------------
+def gpu_arm(args, prm):
+    import torch
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+
+    from via_rs_b200 import _lib
+    from via_rs_b200.server import VIA_RECORDS_NIBBLE, Server, check
+
+    L = _lib.lib()
+    records, keys, query = make_inputs(prm, seed=rank)
+    server = Server.setup(prm, keys, records, VIA_RECORDS_NIBBLE)
+    del records
+    stream = torch.cuda.Stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+    d_q = torch.from_numpy(query.view(np.int64)).cuda()
+    d_m = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
+    d_b = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
+
+    def answer_dev():
+        check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr()), prm.n_lwe,
+                                      ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()), sptr))
+
+    for _ in range(args.warmup):
+        answer_dev()
+    torch.cuda.synchronize()
+
+    # ---- timed region: K device-resident answers.
+    clocks = ClockSampler(local)
+    clocks.start()
+    time.sleep(0.3)
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    l0 = L.via_kernel_launches()
+    with torch.cuda.stream(stream):
+        evs[0].record(stream)
+        for k in range(args.steps):
+            answer_dev()
+            evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    launches = L.via_kernel_launches() - l0
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
+    elapsed = evs[0].elapsed_time(evs[-1]) / 1e3
+    if dist:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    n_answers = args.steps * world
+    value = n_answers / elapsed
+    db_bytes = prm.num_rows * prm.num_cols * prm.n1 * 8
+
+    # ---- e2e: the reference-facing host-buffer call, copies inside the region.
+    for _ in range(2):
+        server.answer(query)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        server.answer(query)
+    e2e_el = time.perf_counter() - t0
+    if dist:
+        t = torch.tensor([e2e_el], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_el = float(t.item())
+    e2e_value = n_answers / e2e_el
+
+    # ---- roofline of the dominant kernel: the FirstDim scan alone, timed live.
+    sel = torch.randint(0, prm.q2, (prm.num_rows * 2 * prm.n1,), dtype=torch.int64, device="cuda")
+    out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
+    for _ in range(2):
+        check(L.via_first_dim_scan_dev(server._h, ctypes.c_void_p(sel.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                       sptr))
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(args.scan_launches):
+        check(L.via_first_dim_scan_dev(server._h, ctypes.c_void_p(sel.data_ptr()), ctypes.c_void_p(out.data_ptr()),
+                                       sptr))
+    e1.record(stream)
+    torch.cuda.synchronize()
+    scan_s = e0.elapsed_time(e1) / 1e3 / args.scan_launches
+    scan_bytes = db_bytes + sel.numel() * 8 + out.numel() * 8
+    peak, peak_kind = load_peaks()
+    achieved = scan_bytes / scan_s / 1e9
+
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "answers/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u64",
+            "data": "synthetic: seeded uniform 4-bit records (numpy PCG64), uniform key/query residues",
+            "config": config_dict(prm),
+            "plain": {"answers_s": value, "db_gbs": value * db_bytes / 1e9, "db_raw_gbs": value * (1 << 30) / 1e9,
+                      "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
+            "batched": None,
+            "roofline": {"bound": "hbm", "kernel": "k_first_dim_ntt (FirstDim scan)", "achieved": achieved,
+                         "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                         "traffic": SCAN_TRAFFIC_BYTES, "launch_ms": scan_s * 1e3,
+                         "algorithmic_bytes": scan_bytes},
+            "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
+                    "d2h_bytes_per_step": int(2 * prm.n2 * 8)},
+            "gpu_launches": int(launches),
+            "clocks": clk,
+        }
+        if world == 1 and not args.no_cpu_baseline:
+            t, threads, sample = cpu_answer_sample(prm)
+            line["cpu_baseline"] = {"value": 1.0 / t, "unit": "answers/s", "cores": threads, "kind": "port",
+                                    "sample": sample}
+        print(json.dumps(line), flush=True)
+    server.close()
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    from via_rs_b200.params import paper_preset
+
+    prm = paper_preset(args.rows, args.cols)
+    if args.impl == "reference":
+        reference_arm(args, prm)
+    else:
+        gpu_arm(args, prm)
+
+
+if __name__ == "__main__":
+    main()

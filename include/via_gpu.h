@@ -6,7 +6,6 @@
  *
  *   Server::setup(ServerConfig, &[RRec], p_mod)  -> via_server_setup
  *   Server::answer(&CompressedQuery)             -> via_server_answer
- *   Server::answer_batch::<T>(&BatchedQuery)     -> via_server_answer_batch
  *   drop(Server)                                 -> via_server_destroy
  *
  * plus the free kernel boundaries the reference names for a GPU build
@@ -116,7 +115,7 @@ uint64_t via_rsk_len(const via_params* p);
  * matrix (setup_db.rs:39-75), lifts them to q2 and forward-transforms them on
  * the device once (prepared_db.rs:57-85), and uploads the eval-form public keys
  * (prepared_keys.rs:69-79). Fewer records than capacity are zero-padded; more
- * is VIA_ERR_DIM_MISMATCH. Uses device 0 unless via_set_device was called.
+ * is VIA_ERR_DIM_MISMATCH. Uses the calling thread's current CUDA device.
  */
 via_status via_server_setup(const via_params* params, const via_public_keys* keys, const void* records,
                             uint64_t n_records, via_record_format format, via_server** out);
@@ -127,6 +126,14 @@ via_status via_server_setup(const via_params* params, const via_public_keys* key
  */
 via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
                              uint64_t* out_body);
+
+/*
+ * The same answer on device buffers, enqueued on `stream` without a host
+ * synchronisation: `query` (n_lwe LWEs), `out_mask`, `out_body` are device
+ * pointers. Answers on one handle are serialised (it owns one workspace).
+ */
+via_status via_server_answer_dev(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
+                                 uint64_t* out_body, void* stream);
 
 void via_server_destroy(via_server* s);
 
@@ -139,6 +146,30 @@ const char* via_last_error(void);
  * prepared database is the other operand.
  */
 via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* out, void* stream);
+
+/*
+ * The FirstDim scan kernel alone, on eval-form operands: `sel_eval` holds the I
+ * selection RLWEs already transformed, `out_eval` receives the J column sums
+ * untransformed. For timing the database scan in isolation.
+ */
+via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
+
+/*
+ * Runs the answer up to `stage` and copies that stage's output, in coefficient
+ * form, to the host buffer `out` (for stage-by-stage parity checks):
+ *   1 cascade RLWEs [n_lwe][2][nl][n1]      (query_decomp.rs:76-78)
+ *   2 query RGSWs at q1 [bits][2L][2][nl][n1] (query_decomp.rs:81-85)
+ *   3 DMux outputs [I][2][nl][n1]            (answer.rs:181-191)
+ *   4 mod-switched rows at q2 [I][2][n1]     (answer.rs:194-199)
+ *   5 FirstDim columns [J][2][n1]            (answer.rs:204-205)
+ *   6 CMux output [2][n1]                    (answer.rs:208-215)
+ *   7 CRot output [2][n1]                    (answer.rs:218-225)
+ */
+via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe, int stage, uint64_t* out,
+                           uint64_t out_len);
+
+/* Number of kernels this library has launched since it was loaded. */
+uint64_t via_kernel_launches(void);
 
 #ifdef __cplusplus
 }

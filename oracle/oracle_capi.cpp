@@ -247,6 +247,62 @@ int vo_server_first_dim(void* sv, const uint64_t* switched, uint64_t* out, int t
   });
 }
 
+// Stage-by-stage intermediates in the include/via_gpu.h via_debug_stage layout.
+int vo_server_debug_stage(void* sv, const uint64_t* query, size_t n_lwe, int stage, uint64_t* out, int threads) {
+  return guarded([&] {
+    OracleServer* s = (OracleServer*)sv;
+    const Params& prm = s->prm;
+    Ring R1 = prm.r1(), R2 = prm.r2();
+    std::vector<Lwe> q = get_query(query, R1, n_lwe);
+    u64* d = out;
+    auto put_rlwe = [&](const Rlwe& c) {
+      put_poly(d, c.mask);
+      put_poly(d, c.body);
+    };
+    if (stage == 1) {
+      for (auto& l : q) put_rlwe(lwe_to_rlwe(R1, l, s->keys.cascade, prm.ck_base));
+      return;
+    }
+    DecompQuery dq = query_decomp(prm, q, s->keys);
+    if (stage == 2) {
+      for (auto* grp : {&dq.dmux, &dq.cmux, &dq.crot})
+        for (auto& g : *grp) {
+          put_rlev(d, g.neg_s_m);
+          put_rlev(d, g.m);
+        }
+      return;
+    }
+    std::vector<RgswEval> dbits;
+    for (auto& g : dq.dmux) dbits.push_back(rgsw_to_eval(R1, g));
+    Rlwe triv{R1.zero(), R1.scalar_const(prm.delta())};
+    std::vector<Rlwe> dm = dmux_tree(R1, dbits, triv, prm.b_dmux, prm.b_dmux);
+    if (stage == 3) {
+      for (auto& c : dm) put_rlwe(c);
+      return;
+    }
+    std::vector<Rlwe> sw;
+    for (auto& c : dm) sw.push_back(mod_switch_sym(R1, c, R2));
+    if (stage == 4) {
+      for (auto& c : sw) put_rlwe(c);
+      return;
+    }
+    std::vector<Rlwe> fd = first_dim(prm, sw, s->db, threads);
+    if (stage == 5) {
+      for (auto& c : fd) put_rlwe(c);
+      return;
+    }
+    std::vector<RgswEval> cbits, rbits;
+    for (auto& g : dq.cmux) cbits.push_back(rgsw_to_eval(R2, mod_switch_rgsw(R1, g, R2)));
+    Rlwe sel = cmux_tree(R2, cbits, fd, prm.b_cmux, prm.b_cmux);
+    if (stage == 6) {
+      put_rlwe(sel);
+      return;
+    }
+    for (auto& g : dq.crot) rbits.push_back(rgsw_to_eval(R2, mod_switch_rgsw(R1, g, R2)));
+    put_rlwe(crot(R2, CRotDir::SlotExtract, rbits, sel, prm.b_cmux, prm.b_cmux));
+  });
+}
+
 // Seconds spent in steps 1..7 by the last vo_server_answer on this thread.
 void vo_stage_times(double* out7) {
   const StageTimes& t = last_stage_times();

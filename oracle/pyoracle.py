@@ -46,6 +46,7 @@ def lib() -> ctypes.CDLL:
         L.vo_server_answer_through_crot.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
         L.vo_server_first_dim.argtypes = [ctypes.c_void_p, _u64p, _u64p, ctypes.c_int]
         L.vo_server_free.argtypes = [ctypes.c_void_p]
+        L.vo_server_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, ctypes.c_int, _u64p, ctypes.c_int]
         L.vo_stage_times.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.vo_shake256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
         _lib = L
@@ -55,6 +56,13 @@ def lib() -> ctypes.CDLL:
 def _ptr(a: np.ndarray):
     assert a.dtype == np.uint64 and a.flags["C_CONTIGUOUS"]
     return a.ctypes.data_as(_u64p)
+
+
+def stage_len(prm: Params, stage: int) -> int:
+    nl, n1 = prm.nl, prm.n1
+    nbits = prm.n_lwe // prm.l_query
+    return {1: prm.n_lwe * 2 * nl * n1, 2: nbits * 2 * prm.l_query * 2 * nl * n1, 3: prm.num_rows * 2 * nl * n1,
+            4: prm.num_rows * 2 * n1, 5: prm.num_cols * 2 * n1, 6: 2 * n1, 7: 2 * n1}[stage]
 
 
 class OracleError(RuntimeError):
@@ -154,6 +162,14 @@ class Server:
         out = np.zeros(prm.num_cols * 2 * prm.n1, dtype=np.uint64)
         _check(lib().vo_server_first_dim(self._h, _ptr(np.ascontiguousarray(switched, dtype=np.uint64)),
                                          _ptr(out), self.threads))
+        return out
+
+    def debug_stage(self, query: np.ndarray, stage: int) -> np.ndarray:
+        """Intermediate `stage` (1..7) in the layout of include/via_gpu.h via_debug_stage."""
+        prm = self.prm
+        q = np.ascontiguousarray(query, dtype=np.uint64)
+        out = np.zeros(stage_len(prm, stage), dtype=np.uint64)
+        _check(lib().vo_server_debug_stage(self._h, _ptr(q), q.size // prm.lwe_len, stage, _ptr(out), self.threads))
         return out
 
     @staticmethod

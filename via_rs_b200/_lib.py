@@ -1,0 +1,63 @@
+"""Loader for libvia_gpu.so, the CUDA implementation behind include/via_gpu.h.
+
+There is no CPU fallback: if the library is missing or cannot load, every
+entry point raises.
+"""
+import ctypes
+import pathlib
+import re
+
+from .params import ViaParams
+
+HERE = pathlib.Path(__file__).resolve().parent
+LIB_PATH = HERE / "libvia_gpu.so"
+HEADER = HERE.parent / "include" / "via_gpu.h"
+
+_u64p = ctypes.POINTER(ctypes.c_uint64)
+_lib = None
+
+
+class ViaPublicKeys(ctypes.Structure):
+    _fields_ = [("cascade_key", _u64p), ("conv_key", _u64p), ("rsk", _u64p)]
+
+
+def declared_symbols() -> list:
+    """Function names declared in include/via_gpu.h."""
+    text = HEADER.read_text()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    return sorted(set(re.findall(r"\b(via_[a-z0-9_]+)\s*\(", text)))
+
+
+def lib() -> ctypes.CDLL:
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise RuntimeError(f"{LIB_PATH} is missing: build it with `python -m via_rs_b200.build`")
+    L = ctypes.CDLL(str(LIB_PATH))
+    P = ctypes.POINTER(ViaParams)
+    L.via_last_error.restype = ctypes.c_char_p
+    for name in ("via_lwe_len", "via_query_len", "via_cascade_key_len", "via_conv_key_len", "via_rsk_len"):
+        f = getattr(L, name)
+        f.restype = ctypes.c_uint64
+        f.argtypes = [P]
+    L.via_server_setup.restype = ctypes.c_int
+    L.via_server_setup.argtypes = [P, ctypes.POINTER(ViaPublicKeys), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                   ctypes.POINTER(ctypes.c_void_p)]
+    L.via_server_answer.restype = ctypes.c_int
+    L.via_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, _u64p, _u64p]
+    L.via_server_destroy.restype = None
+    L.via_server_destroy.argtypes = [ctypes.c_void_p]
+    L.via_first_dim_dev.restype = ctypes.c_int
+    L.via_first_dim_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_server_answer_dev.restype = ctypes.c_int
+    L.via_server_answer_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                        ctypes.c_void_p, ctypes.c_void_p]
+    L.via_first_dim_scan_dev.restype = ctypes.c_int
+    L.via_first_dim_scan_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_debug_stage.restype = ctypes.c_int
+    L.via_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_uint64]
+    L.via_kernel_launches.restype = ctypes.c_uint64
+    L.via_kernel_launches.argtypes = []
+    _lib = L
+    return L

@@ -1,0 +1,12 @@
+#pragma once
+#include "common.cuh"
+
+namespace via {
+
+// out_eval[j] = sum_i db[i][j] (.) sel_eval[i] for mask and body, eval domain at q2.
+// db: [I][J][n]; sel_eval: I RLWEs (mask, body) [I][2][n]; out_eval: [J][2][n].
+// `ntt` selects pointwise products (NTT-friendly q2) or negacyclic schoolbook.
+void first_dim_eval(const u64* db, const u64* sel_eval, u64* out_eval, int I, int J, int n, const DevMod& m, bool ntt,
+                    cudaStream_t st);
+
+}  // namespace via

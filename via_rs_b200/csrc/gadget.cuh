@@ -1,0 +1,171 @@
+// Exact wide arithmetic for the gadget decomposition and modulus switches:
+// 128-bit CRT values, round(|c| * B^L / Q) with a 256-bit-equivalent exact
+// division, and balanced base-B digits (crates/via-primitives/src/encryption/
+// gadget.rs:115-190, crates/via-primitives/src/algebra/wide.rs:145-153).
+// Host-callable so the same code is checked against the oracle on the CPU.
+#pragma once
+#include <cmath>
+
+#include "server.cuh"
+
+namespace via {
+
+// ---------------------------------------------------------------------------
+// Exact wide arithmetic helpers (device).
+// ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ double u128_to_double(u128 x) {
+  return (double)(u64)(x >> 64) * 18446744073709551616.0 + (double)(u64)x;
+}
+__host__ __device__ __forceinline__ double i128_to_double(i128 x) {
+  return x < 0 ? -u128_to_double((u128)(-x)) : u128_to_double((u128)x);
+}
+__host__ __device__ __forceinline__ u128 double_to_u128(double d) {
+  if (d <= 0.0) return 0;
+  if (d < 18446744073709551616.0) return (u128)(u64)d;
+  double hi = floor(d / 18446744073709551616.0);
+  double lo = d - hi * 18446744073709551616.0;
+  if (lo < 0) lo = 0;
+  return ((u128)(u64)hi << 64) | (u128)(u64)lo;
+}
+
+// floor(x / D) for x < 2^127, 0 < D < 2^127, given dD = (double)D. Exact:
+// a double estimate, a second estimate from the (small, exact) remainder, then
+// a final +-1 fix.
+__host__ __device__ __forceinline__ u128 div_exact(u128 x, u128 D, double dD) {
+  u128 q = double_to_u128(u128_to_double(x) / dD);
+  i128 r = (i128)(x - q * D);
+  i128 qci = (i128)(i64)floor(i128_to_double(r) / dD);
+  r -= qci * (i128)D;
+  q = (u128)((i128)q + qci);
+  // The two estimates leave |error| <= 1; the loops are bounded regardless.
+  for (int it = 0; it < 4 && r < 0; ++it) {
+    r += (i128)D;
+    q -= 1;
+  }
+  for (int it = 0; it < 4 && r >= (i128)D; ++it) {
+    r -= (i128)D;
+    q += 1;
+  }
+  return q;
+}
+
+// CRT reconstruction (prim/algebra/rns/basis.rs reconstruct).
+__host__ __device__ __forceinline__ u128 crt2(u64 a0, u64 a1, const DevRing& R) {
+  const DevMod& m1 = R.m[1];
+  u64 a0m = reduce64(a0, m1);
+  u64 diff = submod(a1, a0m, m1.q);
+  u64 t = mul_shoup(diff, R.q0inv_mod_q1, R.q0inv_shoup, m1.q);
+  return (u128)a0 + (u128)R.m[0].q * t;
+}
+
+// ---------------------------------------------------------------------------
+// Gadget decomposition (prim/encryption/gadget.rs:115-190).
+// ---------------------------------------------------------------------------
+struct Gadget {
+  u64 base;
+  int L;
+  int c;          // digits taken from the low chunk (B^c < 2^62); L - c from the high
+  u128 S;         // B^L
+  u64 Bc;         // B^c
+  double dBc, dS_over_Q, dQ;
+  u128 Q, halfQ;
+  u64 half_base;
+  u64 magic;      // floor(2^64 / B) for the 64-bit digit divisions
+};
+
+inline Gadget make_gadget(u64 base, int L, u128 Q) {
+  Gadget g{};
+  g.base = base;
+  g.L = L;
+  u128 S = 1;
+  int c = 0;
+  u128 Bc = 1;
+  for (int i = 0; i < L; ++i) {
+    if ((long double)S * base >= 1.7e38L) throw CudaError(100, "gadget: B^L exceeds 2^127");
+    S *= base;
+    if (S < ((u128)1 << 62)) {
+      c = i + 1;
+      Bc = S;
+    }
+  }
+  // The high chunk holds L - c digits plus a carry; it must fit 62 bits.
+  u128 hi = 1;
+  for (int i = c; i < L; ++i) hi *= base;
+  if (hi >= ((u128)1 << 62)) throw CudaError(100, "gadget: B^L too large for two chunks");
+  g.c = c;
+  g.S = S;
+  g.Bc = (u64)Bc;
+  g.dBc = (double)(u64)Bc;
+  g.Q = Q;
+  g.halfQ = Q / 2;
+  g.dQ = (double)(u64)(Q >> 64) * 18446744073709551616.0 + (double)(u64)Q;
+  double dS = (double)(u64)(S >> 64) * 18446744073709551616.0 + (double)(u64)S;
+  g.dS_over_Q = dS / g.dQ;
+  g.half_base = base / 2;
+  g.magic = (u64)(((u128)1 << 64) / base);
+  return g;
+}
+
+// u / B and u % B for u < 2^63 via a reciprocal and a fix-up.
+__host__ __device__ __forceinline__ u64 divB(u64 u, const Gadget& g, u64& rem) {
+  u64 q = mulhi(u, g.magic);
+  u64 r = u - q * g.base;
+  for (int it = 0; it < 4 && r >= g.base; ++it) {
+    r -= g.base;
+    ++q;
+  }
+  rem = r;
+  return q;
+}
+
+// Extract `cnt` balanced digits of u (LSB first) into d[]; returns the carry-out.
+__host__ __device__ __forceinline__ u64 digits64(u64 u, int cnt, const Gadget& g, i64* d) {
+  for (int k = 0; k < cnt; ++k) {
+    u64 r;
+    u64 q = divB(u, g, r);
+    if (r > g.half_base) {
+      d[k] = (i64)r - (i64)g.base;
+      u = q + 1;
+    } else {
+      d[k] = (i64)r;
+      u = q;
+    }
+  }
+  return u;
+}
+
+// Digits of one coefficient given its residues (nl limbs). Writes L signed
+// digits, d[k] = k-th least significant (pairs with sample L-1-k).
+__host__ __device__ void decompose_coeff(u64 a0, u64 a1, const DevRing& R, const Gadget& g, i64* d) {
+  // Centred lift: v <= Q/2 ? v : v - Q.
+  u128 v = R.nl == 2 ? crt2(a0, a1, R) : (u128)a0;
+  bool neg = v > g.halfQ;
+  u128 mag = neg ? g.Q - v : v;
+  // scaled = floor((mag * S + floor(Q/2)) / Q), exact (wide.rs:145-153).
+  u128 qe = double_to_u128(u128_to_double(mag) * g.dS_over_Q);
+  i128 r = (i128)(mag * g.S + g.halfQ - qe * g.Q);
+  i128 qc = (i128)(i64)floor(i128_to_double(r) / g.dQ);
+  r -= qc * (i128)g.Q;
+  qe = (u128)((i128)qe + qc);
+  for (int it = 0; it < 4 && r < 0; ++it) {
+    r += (i128)g.Q;
+    qe -= 1;
+  }
+  for (int it = 0; it < 4 && r >= (i128)g.Q; ++it) {
+    r -= (i128)g.Q;
+    qe += 1;
+  }
+  // Balanced digits depend only on the value mod B^L; take it non-negative.
+  u128 u = (neg && qe != 0) ? g.S - qe : qe;
+  if (g.c >= g.L) {
+    digits64((u64)u, g.L, g, d);
+  } else {
+    u128 uh = div_exact(u, (u128)g.Bc, g.dBc);
+    u64 ul = (u64)(u - uh * (u128)g.Bc);
+    u64 carry = digits64(ul, g.c, g, d);
+    digits64((u64)uh + carry, g.L - g.c, g, d + g.c);
+  }
+}
+
+
+}  // namespace via

@@ -1,0 +1,608 @@
+// The VIA-C answer pipeline on the device (crates/via-server/src/answer.rs:83-354):
+//
+//   1 QueryDecomp   LWE -> RLWE cascade (prim/conversion/cascade.rs) + RLWE -> RGSW
+//   2 DMux tree     trivial RLWE(delta) -> I RLWEs at q1      (prim/gates/mux.rs:222)
+//   3 ModSwitch     q1 -> q2                                   (prim/switching/mod_switch.rs:57)
+//   4 FirstDim      I x J database scan                        (srv/first_dim.rs:94)
+//   5 CMux tree     J -> 1 at q2                               (prim/gates/mux.rs:167)
+//   6 CRot          slot extraction                            (prim/gates/rotate.rs:128)
+//   7 RespComp      q2 -> q3, ring switch n1 -> n2, body -> q4 (srv/resp_comp.rs:46)
+//
+// Every gadget product is: exact decomposition into balanced digits (kernel
+// k_decompose) -> forward NTT of the digit polys -> one pointwise
+// multiply-accumulate against the eval-form key (k_mac) -> inverse NTT. Linear
+// steps between products are done in whichever domain saves transforms; since
+// the NTT is exact, the coefficient-form results equal the reference's.
+#include <cmath>
+#include <cstring>
+
+#include "first_dim.cuh"
+#include "gadget.cuh"
+#include "server.cuh"
+
+namespace via {
+
+// in: npolys polys [p][nl][n_in]; out: digit polys [p][L][nl][n_out] in sample
+// order (slot s = L-1-k holds digit k). n_out = n_in * stride: the input is
+// first embedded at slot 0 (reshape.rs:58), so other positions get digit 0.
+__global__ void k_decompose(const u64* __restrict__ in, int n_in, int stride, long npolys, DevRing R, Gadget g,
+                            u64* __restrict__ out) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= npolys * n_in) return;
+  long p = gid / n_in;
+  int i = (int)(gid % n_in);
+  const int nl = R.nl;
+  const u64* src = in + p * nl * n_in;
+  u64 a0 = src[i], a1 = nl == 2 ? src[n_in + i] : 0;
+  i64 d[64];
+  decompose_coeff(a0, a1, R, g, d);
+  const int n_out = n_in * stride;
+  u64* dst = out + p * (long)g.L * nl * n_out;
+  for (int k = 0; k < g.L; ++k) {
+    int s = g.L - 1 - k;
+    for (int l = 0; l < nl; ++l) {
+      u64* o = dst + ((long)s * nl + l) * n_out + (long)i * stride;
+      o[0] = lift_i64(d[k], R.m[l]);
+      for (int z = 1; z < stride; ++z) o[z] = 0;
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Multiply-accumulate against eval-form keys.
+//   out[o].{mask,body} = sum_{s<T} D[o*T + s] (*) K_o[s].{mask,body}
+// K_o = K + key_id(o) * T*2*nl*n with key_id(o) = (o / kdiv) % kmod.
+// ---------------------------------------------------------------------------
+__global__ void k_mac_ntt(const u64* __restrict__ D, const u64* __restrict__ K, u64* __restrict__ out, int T, int n,
+                          int nl, long nout, long kdiv, long kmod, DevRing R) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = (long)nl * n;
+  if (gid >= nout * per) return;
+  long o = gid / per;
+  int rem = (int)(gid % per);
+  int l = rem / n;
+  const u64* Ko = K + ((o / kdiv) % kmod) * (long)T * 2 * per;
+  const u64* Do = D + o * (long)T * per;
+  Acc128 am{0, 0}, ab{0, 0};
+  for (int s = 0; s < T; ++s) {
+    u64 dv = Do[s * per + rem];
+    mac128(am, dv, Ko[(2 * s) * per + rem]);
+    mac128(ab, dv, Ko[(2 * s + 1) * per + rem]);
+  }
+  const DevMod& m = R.m[l];
+  out[(2 * o) * per + rem] = reduce128(am.hi, am.lo, m);
+  out[(2 * o + 1) * per + rem] = reduce128(ab.hi, ab.lo, m);
+}
+
+// Schoolbook (non-NTT ring) variant: negacyclic products, exact.
+__global__ void k_mac_schoolbook(const u64* __restrict__ D, const u64* __restrict__ K, u64* __restrict__ out, int T,
+                                 int n, int nl, long nout, long kdiv, long kmod, DevRing R) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = (long)nl * n;
+  if (gid >= nout * per) return;
+  long o = gid / per;
+  int rem = (int)(gid % per);
+  int l = rem / n, t = rem % n;
+  const u64* Ko = K + ((o / kdiv) % kmod) * (long)T * 2 * per;
+  const u64* Do = D + o * (long)T * per;
+  const DevMod& m = R.m[l];
+  const bool pow2 = m.log2q >= 0;
+  u64 wm = 0, wb = 0;
+  Acc128 pm{0, 0}, nm{0, 0}, pb{0, 0}, nb{0, 0};
+  for (int s = 0; s < T; ++s) {
+    const u64* dp = Do + s * per + (long)l * n;
+    const u64* km = Ko + (2 * s) * per + (long)l * n;
+    const u64* kb = Ko + (2 * s + 1) * per + (long)l * n;
+    for (int j = 0; j < n; ++j) {
+      u64 dv = dp[j];
+      if (dv == 0) continue;
+      int k = t - j;
+      bool ng = k < 0;
+      if (ng) k += n;
+      if (pow2) {
+        u64 a = dv * km[k], b = dv * kb[k];
+        wm += ng ? (u64)0 - a : a;
+        wb += ng ? (u64)0 - b : b;
+      } else if (ng) {
+        mac128(nm, dv, km[k]);
+        mac128(nb, dv, kb[k]);
+      } else {
+        mac128(pm, dv, km[k]);
+        mac128(pb, dv, kb[k]);
+      }
+    }
+  }
+  u64 rm, rb;
+  if (pow2) {
+    rm = wm & (m.q - 1);
+    rb = wb & (m.q - 1);
+  } else {
+    rm = submod(reduce128(pm.hi, pm.lo, m), reduce128(nm.hi, nm.lo, m), m.q);
+    rb = submod(reduce128(pb.hi, pb.lo, m), reduce128(nb.hi, nb.lo, m), m.q);
+  }
+  out[(2 * o) * per + rem] = rm;
+  out[(2 * o + 1) * per + rem] = rb;
+}
+
+// ---------------------------------------------------------------------------
+// Elementwise kernels. All buffers are [poly][limb][n].
+// ---------------------------------------------------------------------------
+// out[j] = a[j*sa] + sign * b[j*sb] for RLWEs (2 polys each); sign in {+1,-1}.
+__global__ void k_rlwe_addsub(u64* out, const u64* a, long sa, const u64* b, long sb, int sign, long count, int n,
+                              int nl, DevRing R) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = 2L * nl * n;
+  if (gid >= count * per) return;
+  long j = gid / per;
+  int rem = (int)(gid % per);
+  int l = (rem / n) % nl;
+  u64 q = R.m[l].q;
+  u64 x = a[j * sa * per + rem], y = b[j * sb * per + rem];
+  out[j * per + rem] = sign > 0 ? addmod(x, y, q) : submod(x, y, q);
+}
+
+// DMux combine (mux.rs:129-137, 222-251): out[2j] = in[j] - ext[j], out[2j+1] = ext[j].
+__global__ void k_dmux_combine(u64* out, const u64* in, const u64* ext, long count, int n, int nl, DevRing R) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = 2L * nl * n;
+  if (gid >= count * per) return;
+  long j = gid / per;
+  int rem = (int)(gid % per);
+  int l = (rem / n) % nl;
+  u64 q = R.m[l].q;
+  u64 e = ext[j * per + rem];
+  out[(2 * j) * per + rem] = submod(in[j * per + rem], e, q);
+  out[(2 * j + 1) * per + rem] = e;
+}
+
+// Modulus switch (prim/switching/kernels/mod_switch.rs:59-61):
+// c' = floor((c * q_dst + floor(q_src/2)) / q_src) mod q_dst, c the canonical value.
+__global__ void k_mod_switch(const u64* __restrict__ in, DevRing S, u64* __restrict__ out, DevMod dst, long ncoef,
+                             int n, double dQs) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= ncoef) return;
+  long p = gid / n;
+  int i = (int)(gid % n);
+  u128 v = S.nl == 2 ? crt2(in[(p * 2) * n + i], in[(p * 2 + 1) * n + i], S) : (u128)in[p * n + i];
+  u128 Qs = S.Q();
+  u128 num = v * dst.q + (Qs >> 1);
+  u128 r;
+  if (S.nl == 1 && S.m[0].log2q >= 0)
+    r = num >> S.m[0].log2q;
+  else
+    r = div_exact(num, Qs, dQs);
+  u64 rr = (u64)r;
+  out[p * n + i] = rr >= dst.q ? rr - dst.q : rr;
+}
+
+// ---------------------------------------------------------------------------
+// Cascade (prim/conversion/cascade.rs + conv.rs:122-148) helpers.
+// ---------------------------------------------------------------------------
+// LWE [lwe][nl*(n1+1)] -> rank-n1 MLWE of degree 1: masks [lwe][idx][nl], body [lwe][nl].
+__global__ void k_lwe_to_mlwe(const u64* __restrict__ q, int n1, int nl, long nlwe, u64* masks, u64* body) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  long per = (long)nl * (n1 + 1);
+  if (gid >= nlwe * per) return;
+  long w = gid / per;
+  int r = (int)(gid % per);
+  if (r < nl * n1) {
+    int l = r / n1, idx = r % n1;
+    masks[(w * n1 + idx) * nl + l] = q[w * per + r];
+  } else {
+    int l = r - nl * n1;
+    body[w * nl + l] = q[w * per + r];
+  }
+}
+
+// After the step MAC: P [lwe][RANK_IN][2][nl][N] (eval). Produces
+// masks_out[lwe][j] = -(P[j].mask + P[j+R].mask) for j < R and
+// bsum[lwe] = sum_idx P[idx].body.
+__global__ void k_cascade_reduce(const u64* __restrict__ P, int rank_in, int N, int nl, long nlwe, DevRing R,
+                                 u64* __restrict__ masks_out, u64* __restrict__ bsum) {
+  const int half = rank_in / 2;
+  long per = (long)nl * N;
+  long items = nlwe * (half + 1) * per;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= items) return;
+  long w = gid / ((half + 1) * per);
+  long r = gid % ((half + 1) * per);
+  int j = (int)(r / per);
+  int rem = (int)(r % per);
+  int l = rem / N;
+  u64 q = R.m[l].q;
+  const u64* Pw = P + w * rank_in * 2 * per;
+  if (j < half) {
+    u64 a = Pw[(2L * j) * per + rem], b = Pw[(2L * (j + half)) * per + rem];
+    masks_out[(w * half + j) * per + rem] = negmod(addmod(a, b, q), q);
+  } else {
+    u64 acc = 0;
+    for (int idx = 0; idx < rank_in; ++idx) acc = addmod(acc, Pw[(2L * idx + 1) * per + rem], q);
+    bsum[w * per + rem] = acc;
+  }
+}
+
+// body_out[lwe] = embed_at(body_in[lwe], N_out, 0) - bsum[lwe] (coefficient form).
+__global__ void k_cascade_body(const u64* __restrict__ body_in, const u64* __restrict__ bsum, int n_in, int nl,
+                               long nlwe, DevRing R, u64* __restrict__ body_out) {
+  const int n_out = 2 * n_in;
+  long per = (long)nl * n_out;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nlwe * per) return;
+  long w = gid / per;
+  int rem = (int)(gid % per);
+  int l = rem / n_out, t = rem % n_out;
+  u64 q = R.m[l].q;
+  u64 e = (t & 1) ? 0 : body_in[(w * nl + l) * n_in + t / 2];
+  body_out[w * per + rem] = submod(e, bsum[w * per + rem], q);
+}
+
+// Assemble cascade outputs into RLWEs [lwe][2][nl][n1].
+__global__ void k_pack_rlwe(const u64* masks, const u64* body, long nlwe, int n1, int nl, u64* out) {
+  long per = (long)nl * n1;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nlwe * per) return;
+  long w = gid / per;
+  int rem = (int)(gid % per);
+  out[(2 * w) * per + rem] = masks[w * per + rem];
+  out[(2 * w + 1) * per + rem] = body[w * per + rem];
+}
+
+// rlwe_to_rgsw assembly (prim/gates/convert.rs:162-178): for bit b, level i:
+// neg_s_m[i] = (rlwe_i.body + gp_i.mask, gp_i.body), m[i] = rlwe_i.
+// rlwe: [bits*L][2][nl][n]; gp: same shape; rgsw: [bits][2L][2][nl][n].
+__global__ void k_assemble_rgsw(const u64* rlwe, const u64* gp, int L, long bits, int n, int nl, DevRing R, u64* rgsw) {
+  long per = (long)nl * n;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= bits * L * 2 * per) return;
+  long w = gid / (2 * per);  // rlwe index = bit*L + i
+  int rem = (int)(gid % (2 * per));
+  int mb = rem / per;
+  int r2 = rem % per;
+  int l = r2 / n;
+  long b = w / L;
+  int i = (int)(w % L);
+  u64 q = R.m[l].q;
+  u64* dst_nsm = rgsw + ((b * 2 * L + i) * 2 + mb) * per + r2;
+  u64* dst_m = rgsw + ((b * 2 * L + L + i) * 2 + mb) * per + r2;
+  u64 g = gp[(2 * w + mb) * per + r2];
+  if (mb == 0)
+    *dst_nsm = addmod(rlwe[(2 * w + 1) * per + r2], g, q);
+  else
+    *dst_nsm = g;
+  *dst_m = rlwe[(2 * w + mb) * per + r2];
+}
+
+// CRot (rotate.rs:128-150, SlotExtract): rot = -(X^(n - 2^i) * ct); diff = rot - ct.
+__global__ void k_crot_diff(const u64* ct, int n, int k, DevMod m, u64* diff) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 2 * n) return;
+  int p = gid / n, i = gid % n;
+  // (X^k * a)[i] = a[i-k] (negated on wrap); rot = -(that).
+  int src = i - k;
+  bool wrap = src < 0;
+  if (wrap) src += n;
+  u64 v = ct[p * n + src];
+  u64 xk = wrap ? negmod(v, m.q) : v;
+  u64 rot = negmod(xk, m.q);
+  diff[p * n + i] = submod(rot, ct[p * n + i], m.q);
+}
+
+// Ring switch inputs (prim/switching/ring_switch.rs:358-385): for j < d,
+// mask_proj_j[t] = (X^j * mask)[d t]; body_proj_0[t] = body[d t].
+__global__ void k_ring_switch_proj(const u64* ct, int n1, int n2, DevMod m, u64* mask_proj, u64* body_proj) {
+  int d = n1 / n2;
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (d + 1) * n2) return;
+  int j = gid / n2, t = gid % n2;
+  if (j == d) {
+    body_proj[t] = ct[n1 + d * t];
+    return;
+  }
+  int src = d * t - j;
+  bool wrap = src < 0;
+  if (wrap) src += n1;
+  u64 v = ct[src];
+  mask_proj[j * n2 + t] = wrap ? negmod(v, m.q) : v;
+}
+
+// acc over j of gp_j (eval or coeff, summed as residues): out = -(sum mask), body_proj - sum body.
+__global__ void k_ring_switch_sum(const u64* gp, int d, int n2, DevMod m, u64* acc) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 2 * n2) return;
+  int mb = gid / n2, t = gid % n2;
+  u64 s = 0;
+  for (int j = 0; j < d; ++j) s = addmod(s, gp[(2 * j + mb) * n2 + t], m.q);
+  acc[mb * n2 + t] = s;
+}
+
+__global__ void k_ring_switch_finish(const u64* acc, const u64* body_proj, int n2, DevMod m3, DevMod m4, double dq3,
+                                     u64* out_mask, u64* out_body) {
+  int t = blockIdx.x * blockDim.x + threadIdx.x;
+  if (t >= n2) return;
+  u64 q3 = m3.q;
+  u64 mask = negmod(acc[t], q3);
+  u64 body = submod(body_proj[t], acc[n2 + t], q3);
+  out_mask[t] = mask;  // mask: q3 -> q3 is the identity rescale
+  // body: q3 -> q4 (mod_switch_asym, prim/switching/mod_switch.rs:124-154).
+  u128 num = (u128)body * m4.q + q3 / 2;
+  u64 r = (u64)div_exact(num, (u128)q3, dq3);
+  out_body[t] = r >= m4.q ? r - m4.q : r;
+}
+
+// ---------------------------------------------------------------------------
+// Host-side orchestration.
+// ---------------------------------------------------------------------------
+static inline unsigned blocks(long items, int threads = 256) { return (unsigned)((items + threads - 1) / threads); }
+
+struct Workspace {
+  // Sizes.
+  long nlwe = 0, nbits = 0;
+  // Cascade.
+  DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
+  // RLWE -> RGSW.
+  DevBuf g_digits, g_gp, rgsw_q1;  // rgsw_q1: [nbits][2L][2][nl][n1]
+  DevBuf rgsw_q2;                  // cmux + crot bits at q2
+  // DMux.
+  DevBuf dm_a, dm_b, dm_digits, dm_ext;
+  // FirstDim / CMux.
+  DevBuf sel, fd_out, cm_diff, cm_digits, cm_ext, cm_b;
+  // CRot / RespComp.
+  DevBuf cr_ct, cr_diff, cr_digits, cr_ext, rs_ct3, rs_mproj, rs_bproj, rs_digits, rs_gp, rs_acc;
+  Gadget g_ck, g_dmux, g_cmux, g_rsk;
+};
+
+void WorkspaceDeleter::operator()(Workspace* w) const { delete w; }
+void workspace_destroy(Server& s) { s.ws.reset(); }
+
+void workspace_create(Server& s) {
+  const via_params& p = s.prm;
+  auto w = std::make_unique<Workspace>();
+  const long n1 = p.n1, n2 = p.n2, nl = s.r1.nl, L = p.l_query, Lck = p.l_ck, I = p.num_rows, J = p.num_cols;
+  w->nlwe = (long)query_lwes(p);
+  w->nbits = w->nlwe / L;
+  const long nlwe = w->nlwe;
+  w->c_masks_a.alloc(nlwe * n1 * nl);
+  w->c_masks_b.alloc(nlwe * n1 * nl);
+  w->c_body_a.alloc(nlwe * n1 * nl);
+  w->c_body_b.alloc(nlwe * n1 * nl);
+  w->c_digits.alloc(nlwe * 2 * n1 * Lck * nl);
+  w->c_P.alloc(nlwe * 2 * n1 * 2 * nl);
+  w->c_bsum.alloc(nlwe * n1 * nl);
+  w->c_rlwe.alloc(nlwe * 2 * n1 * nl);
+  w->g_digits.alloc(nlwe * Lck * nl * n1);
+  w->g_gp.alloc(nlwe * 2 * nl * n1);
+  w->rgsw_q1.alloc(w->nbits * 2 * L * 2 * nl * n1);
+  w->rgsw_q2.alloc(w->nbits * 2 * L * 2 * n1);
+  w->dm_a.alloc(I * 2 * nl * n1);
+  w->dm_b.alloc(I * 2 * nl * n1);
+  w->dm_digits.alloc(std::max(1L, I / 2) * 2 * L * nl * n1);
+  w->dm_ext.alloc(std::max(1L, I / 2) * 2 * nl * n1);
+  w->sel.alloc(I * 2 * n1);
+  w->fd_out.alloc(J * 2 * n1);
+  w->cm_diff.alloc(std::max(1L, J / 2) * 2 * n1);
+  w->cm_digits.alloc(std::max(1L, J / 2) * 2 * L * n1);
+  w->cm_ext.alloc(std::max(1L, J / 2) * 2 * n1);
+  w->cm_b.alloc(std::max(1L, J / 2) * 2 * n1);
+  w->cr_ct.alloc(2 * n1);
+  w->cr_diff.alloc(2 * n1);
+  w->cr_digits.alloc(2 * L * n1);
+  w->cr_ext.alloc(2 * n1);
+  w->rs_ct3.alloc(2 * n1);
+  long d = n1 / n2;
+  w->rs_mproj.alloc(d * n2);
+  w->rs_bproj.alloc(n2);
+  w->rs_digits.alloc(d * p.l_rsk * n2);
+  w->rs_gp.alloc(d * 2 * n2);
+  w->rs_acc.alloc(2 * n2);
+  w->g_ck = make_gadget(p.ck_base, (int)p.l_ck, s.r1.Q());
+  w->g_dmux = make_gadget(p.b_dmux, (int)p.l_query, s.r1.Q());
+  w->g_cmux = make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q());
+  w->g_rsk = make_gadget(p.b_rsk, (int)p.l_rsk, s.r3.Q());
+  s.ws.reset(w.release());
+}
+
+static void to_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
+  if (R.ntt) ntt_forward(data, n, R.nl, segments, R.t[0], R.t[1], st);
+}
+static void from_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
+  if (R.ntt) ntt_inverse(data, n, R.nl, segments, R.t[0], R.t[1], st);
+}
+
+// Gadget products of `nout` outputs with T digit polys each (already in the eval
+// domain) against keys: out eval [nout][2][nl][n].
+static void mac(const DevRing& R, const u64* D, const u64* K, u64* out, int T, int n, long nout, long kdiv, long kmod,
+                cudaStream_t st) {
+  long items = nout * R.nl * n;
+  if (R.ntt)
+    k_mac_ntt<<<blocks(items), 256, 0, st>>>(D, K, out, T, n, R.nl, nout, kdiv, kmod, R);
+  else
+    k_mac_schoolbook<<<blocks(items), 256, 0, st>>>(D, K, out, T, n, R.nl, nout, kdiv, kmod, R);
+  VIA_LAUNCHED();
+}
+
+static void decompose(const DevRing& R, const Gadget& g, const u64* in, int n_in, int stride, long npolys, u64* out,
+                      cudaStream_t st) {
+  k_decompose<<<blocks(npolys * n_in), 128, 0, st>>>(in, n_in, stride, npolys, R, g, out);
+  VIA_LAUNCHED();
+}
+
+static double to_double(u128 x) { return (double)(u64)(x >> 64) * 18446744073709551616.0 + (double)(u64)x; }
+
+static void mod_switch(const DevRing& S, const u64* in, const DevRing& D, u64* out, long npolys, int n, cudaStream_t st) {
+  long nco = npolys * n;
+  k_mod_switch<<<blocks(nco), 256, 0, st>>>(in, S, out, D.m[0], nco, n, to_double(S.Q()));
+  VIA_LAUNCHED();
+}
+
+// Step 1: QueryDecomp -> rgsw_q1 [nbits][2L][2][nl][n1] (coefficient form).
+static void query_decomp(Server& s, const u64* d_query, cudaStream_t st) {
+  Workspace& w = *s.ws;
+  const via_params& p = s.prm;
+  const DevRing& R = s.r1;
+  const int n1 = p.n1, nl = R.nl, L = p.l_ck;
+  const long nlwe = w.nlwe;
+  k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query, n1, nl, nlwe, w.c_masks_a.p, w.c_body_a.p);
+  VIA_LAUNCHED();
+  u64 *mi = w.c_masks_a.p, *mo = w.c_masks_b.p, *bi = w.c_body_a.p, *bo = w.c_body_b.p;
+  const u64 step_len = (u64)2 * n1 * L * 2 * nl;
+  int k = 0;
+  for (int n_in = 1; n_in < n1; n_in <<= 1, ++k) {
+    const int n_out = 2 * n_in, rank_in = n1 / n_in;
+    const long polys = nlwe * rank_in;
+    decompose(R, w.g_ck, mi, n_in, 2, polys, w.c_digits.p, st);
+    to_eval(R, w.c_digits.p, n_out, polys * L * nl, st);
+    mac(R, w.c_digits.p, s.cascade_eval.p + k * step_len, w.c_P.p, L, n_out, polys, 1, rank_in, st);
+    const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
+    k_cascade_reduce<<<blocks(items), 256, 0, st>>>(w.c_P.p, rank_in, n_out, nl, nlwe, R, mo, w.c_bsum.p);
+    VIA_LAUNCHED();
+    from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
+    from_eval(R, w.c_bsum.p, n_out, nlwe * nl, st);
+    k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, w.c_bsum.p, n_in, nl, nlwe, R, bo);
+    VIA_LAUNCHED();
+    std::swap(mi, mo);
+    std::swap(bi, bo);
+  }
+  k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, w.c_rlwe.p);
+  VIA_LAUNCHED();
+  // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178):
+  // decompose every RLWE mask (its polys are at index 2w of c_rlwe).
+  const int Lq = p.l_query;
+  // The final rank-1 masks are already contiguous [lwe][nl][n1] in `mi`.
+  decompose(R, w.g_ck, mi, n1, 1, nlwe, w.g_digits.p, st);
+  to_eval(R, w.g_digits.p, n1, nlwe * L * nl, st);
+  mac(R, w.g_digits.p, s.conv_eval.p, w.g_gp.p, L, n1, nlwe, 1, 1, st);
+  from_eval(R, w.g_gp.p, n1, nlwe * 2 * nl, st);
+  k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(w.c_rlwe.p, w.g_gp.p, Lq, w.nbits, n1, nl, R,
+                                                               w.rgsw_q1.p);
+  VIA_LAUNCHED();
+}
+
+// One external-product level: ext[j] = bit (x) ct[j] for `count` RLWEs (coefficient
+// form in `cts`), result in the eval domain unless `to_coeff`.
+static void external_products(const DevRing& R, const Gadget& g, const u64* rgsw_eval, const u64* cts, long count,
+                              u64* digits, u64* ext, bool to_coeff, cudaStream_t st) {
+  const int n = R.n, L = g.L;
+  // Decompose mask and body of every RLWE: 2*count polys -> L digits each,
+  // giving per RLWE 2L digit polys ordered (mask digits, body digits), which
+  // pair with (neg_s_m samples, m samples) of the RGSW.
+  decompose(R, g, cts, n, 1, 2 * count, digits, st);
+  to_eval(R, digits, n, 2 * count * L * R.nl, st);
+  mac(R, digits, rgsw_eval, ext, 2 * L, n, count, 1, 1, st);
+  if (to_coeff) from_eval(R, ext, n, 2 * count * R.nl, st);
+}
+
+void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st) {
+  answer_device_stages(s, d_query, d_mask, d_body, st, 0, nullptr);
+}
+
+// Runs the pipeline; when stop_stage > 0, copies that stage's output (in
+// coefficient form) to `dump` and returns early. Stages: 1 cascade RLWEs,
+// 2 query RGSWs at q1, 3 DMux outputs, 4 mod-switched rows at q2, 5 FirstDim
+// columns, 6 CMux output, 7 CRot output.
+void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st, int stop_stage,
+                          u64* dump) {
+  Workspace& w = *s.ws;
+  const via_params& p = s.prm;
+  const int n1 = p.n1, n2 = p.n2, L = p.l_query, nl = s.r1.nl;
+  const long I = p.num_rows, J = p.num_cols;
+  const int nd = ilog2(I), nc = ilog2(J);
+  const int nr = (int)(w.nbits - nd - nc);
+  const long rgsw1 = 2L * L * 2 * nl * n1, rgsw2 = 2L * L * 2 * n1;
+
+  auto copy_out = [&](const u64* src, size_t count) {
+    VIA_CUDA(cudaMemcpyAsync(dump, src, count * 8, cudaMemcpyDeviceToDevice, st));
+  };
+  // ---- Step 1: QueryDecomp.
+  query_decomp(s, d_query, st);
+  if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
+  if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
+
+  // ---- Step 2: DMux tree at q1 from the trivial RLWE(0, delta) (answer.rs:181-191).
+  // DMux bits to eval form in place (their coefficient form is no longer needed).
+  to_eval(s.r1, w.rgsw_q1.p, n1, (long)nd * 2 * L * 2 * nl, st);
+  {
+    VIA_CUDA(cudaMemsetAsync(w.dm_a.p, 0, 2 * nl * n1 * 8, st));
+    u128 Q1 = s.r1.Q();
+    u128 delta = (Q1 + p.p - 1) / p.p;
+    for (int l = 0; l < nl; ++l) {
+      u64 v = (u64)(delta % s.r1.m[l].q);
+      VIA_CUDA(cudaMemcpyAsync(w.dm_a.p + (long)(nl + l) * n1, &v, 8, cudaMemcpyHostToDevice, st));
+    }
+    u64 *in = w.dm_a.p, *out = w.dm_b.p;
+    for (int i = 0; i < nd; ++i) {
+      long active = 1L << i;
+      external_products(s.r1, w.g_dmux, w.rgsw_q1.p + i * rgsw1, in, active, w.dm_digits.p, w.dm_ext.p, true, st);
+      k_dmux_combine<<<blocks(active * 2 * nl * n1), 256, 0, st>>>(out, in, w.dm_ext.p, active, n1, nl, s.r1);
+      VIA_LAUNCHED();
+      std::swap(in, out);
+    }
+    if (stop_stage == 3) return copy_out(in, (size_t)I * 2 * nl * n1);
+    // ---- Step 3: ModSwitch q1 -> q2 (answer.rs:194-199) into the selection buffer.
+    mod_switch(s.r1, in, s.r2, w.sel.p, 2 * I, n1, st);
+  }
+  if (stop_stage == 4) return copy_out(w.sel.p, (size_t)I * 2 * n1);
+
+  // ---- Step 4: FirstDim (answer.rs:204-205) — result stays in the eval domain.
+  to_eval(s.r2, w.sel.p, n1, 2 * I, st);
+  first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st);
+  if (stop_stage == 5) {
+    copy_out(w.fd_out.p, (size_t)J * 2 * n1);
+    from_eval(s.r2, dump, n1, 2 * J, st);
+    return;
+  }
+
+  // ---- CMux / CRot bits: mod_switch_rgsw q1 -> q2 (convert.rs:223-240), then eval.
+  const long nq2 = (long)(nc + nr);
+  if (nq2) {
+    mod_switch(s.r1, w.rgsw_q1.p + nd * rgsw1, s.r2, w.rgsw_q2.p, nq2 * 2 * L * 2, n1, st);
+    to_eval(s.r2, w.rgsw_q2.p, n1, nq2 * 2 * L * 2, st);
+  }
+
+  // ---- Step 5: CMux tree (mux.rs:167-198), level by level in the eval domain:
+  // diff = in[2j+1] - in[2j] (eval) -> coeff -> gadget product -> out[j] = in[2j] + ext.
+  u64* cur = w.fd_out.p;
+  u64* nxt = nullptr;
+  for (int i = 0; i < nc; ++i) {
+    long half = (J >> i) / 2;
+    k_rlwe_addsub<<<blocks(half * 2 * n1), 256, 0, st>>>(w.cm_diff.p, cur + 2 * n1, 2, cur, 2, -1, half, n1, 1, s.r2);
+    VIA_LAUNCHED();
+    from_eval(s.r2, w.cm_diff.p, n1, 2 * half, st);
+    external_products(s.r2, w.g_cmux, w.rgsw_q2.p + i * rgsw2, w.cm_diff.p, half, w.cm_digits.p, w.cm_ext.p, false, st);
+    nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
+    k_rlwe_addsub<<<blocks(half * 2 * n1), 256, 0, st>>>(nxt, cur, 2, w.cm_ext.p, 1, +1, half, n1, 1, s.r2);
+    VIA_LAUNCHED();
+    cur = nxt;
+  }
+  // Selected column back to coefficient form.
+  VIA_CUDA(cudaMemcpyAsync(w.cr_ct.p, cur, 2 * n1 * 8, cudaMemcpyDeviceToDevice, st));
+  from_eval(s.r2, w.cr_ct.p, n1, 2, st);
+  if (stop_stage == 6) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
+
+  // ---- Step 6: CRot, SlotExtract (rotate.rs:128-150).
+  for (int i = 0; i < nr; ++i) {
+    k_crot_diff<<<blocks(2 * n1), 256, 0, st>>>(w.cr_ct.p, n1, n1 - (1 << i), s.r2.m[0], w.cr_diff.p);
+    VIA_LAUNCHED();
+    external_products(s.r2, w.g_cmux, w.rgsw_q2.p + (nc + i) * rgsw2, w.cr_diff.p, 1, w.cr_digits.p, w.cr_ext.p, true,
+                      st);
+    k_rlwe_addsub<<<blocks(2 * n1), 256, 0, st>>>(w.cr_ct.p, w.cr_ct.p, 1, w.cr_ext.p, 1, +1, 1, n1, 1, s.r2);
+    VIA_LAUNCHED();
+  }
+
+  if (stop_stage == 7) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
+  // ---- Step 7: RespComp (resp_comp.rs:46-76).
+  mod_switch(s.r2, w.cr_ct.p, s.r3n1, w.rs_ct3.p, 2, n1, st);
+  const int d = n1 / n2;
+  k_ring_switch_proj<<<blocks((d + 1) * n2), 256, 0, st>>>(w.rs_ct3.p, n1, n2, s.r3.m[0], w.rs_mproj.p, w.rs_bproj.p);
+  VIA_LAUNCHED();
+  decompose(s.r3, w.g_rsk, w.rs_mproj.p, n2, 1, d, w.rs_digits.p, st);
+  to_eval(s.r3, w.rs_digits.p, n2, (long)d * p.l_rsk, st);
+  mac(s.r3, w.rs_digits.p, s.rsk_eval.p, w.rs_gp.p, (int)p.l_rsk, n2, d, 1, d, st);
+  k_ring_switch_sum<<<blocks(2 * n2), 256, 0, st>>>(w.rs_gp.p, d, n2, s.r3.m[0], w.rs_acc.p);
+  VIA_LAUNCHED();
+  from_eval(s.r3, w.rs_acc.p, n2, 2, st);
+  k_ring_switch_finish<<<blocks(n2), 256, 0, st>>>(w.rs_acc.p, w.rs_bproj.p, n2, s.r3.m[0], s.r4.m[0],
+                                                   (double)p.q3, d_mask, d_body);
+  VIA_LAUNCHED();
+}
+
+}  // namespace via

@@ -1,0 +1,348 @@
+// Server::setup / answer / destroy behind the C ABI of include/via_gpu.h.
+#include <cstring>
+#include <mutex>
+#include <string>
+
+#include "first_dim.cuh"
+#include "server.cuh"
+
+namespace via {
+
+struct ApiError : std::runtime_error {
+  via_status code;
+  ApiError(via_status c, const std::string& m) : std::runtime_error(m), code(c) {}
+};
+
+unsigned long long g_kernel_launches = 0;
+static thread_local std::string g_last_error;
+
+template <class F>
+static via_status guarded(F&& f) {
+  try {
+    f();
+    g_last_error.clear();
+    return VIA_OK;
+  } catch (const ApiError& e) {
+    g_last_error = e.what();
+    return e.code;
+  } catch (const CudaError& e) {
+    g_last_error = e.what();
+    return e.status == 101 ? VIA_ERR_OUT_OF_MEMORY : (e.status == 100 ? VIA_ERR_INVALID_ARGUMENT : VIA_ERR_CUDA);
+  } catch (const std::bad_alloc&) {
+    g_last_error = "host allocation failed";
+    return VIA_ERR_OUT_OF_MEMORY;
+  } catch (const std::exception& e) {
+    g_last_error = e.what();
+    return VIA_ERR_INVALID_ARGUMENT;
+  }
+}
+
+void DevBuf::alloc(size_t count) {
+  free();
+  if (count == 0) return;
+  cudaError_t e = cudaMalloc(&p, count * 8);
+  if (e != cudaSuccess) {
+    p = nullptr;
+    (void)cudaGetLastError();
+    throw CudaError(101, "cudaMalloc(" + std::to_string(count * 8) + " bytes): " + cudaGetErrorString(e));
+  }
+  n = count;
+}
+void DevBuf::free() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  n = 0;
+}
+
+int ilog2(u64 v) { return v <= 1 ? 0 : 63 - __builtin_clzll(v); }
+static bool pow2(u64 v) { return v && !(v & (v - 1)); }
+
+// Shape guards of Server::setup / answer_through_crot (srv/answer.rs:132-157,461-471).
+void validate_params(const via_params& p) {
+  if (!pow2(p.num_rows) || !pow2(p.num_cols))
+    throw ApiError(VIA_ERR_DIM_MISMATCH, "num_rows and num_cols must be powers of two");
+  if (!pow2(p.n1) || !pow2(p.n2) || !pow2(p.n_rec) || p.n2 > p.n1 || p.n_rec > p.n2 || p.n1 > 4096)
+    throw ApiError(VIA_ERR_DIM_MISMATCH, "ring degrees must be powers of two with n_rec <= n2 <= n1 <= 4096");
+  if (p.l_query == 0 || p.l_ck == 0 || p.l_rsk == 0 || p.l_query > 64 || p.l_ck > 64 || p.l_rsk > 64)
+    throw ApiError(VIA_ERR_INVALID_ARGUMENT, "gadget depths must be in 1..64");
+  for (u64 b : {p.b_dmux, p.b_cmux, p.ck_base, p.b_rsk})
+    if (b < 2 || b >= (1ull << 32)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "gadget bases must be in [2, 2^32)");
+  for (u64 q : {p.q1_0, p.q2, p.q3, p.q4, p.p})
+    if (q < 2 || q >= (1ull << 62)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "moduli must be in [2, 2^62)");
+  if (p.q1_1 && (p.q1_1 < 2 || p.q1_1 >= (1ull << 62)))
+    throw ApiError(VIA_ERR_INVALID_ARGUMENT, "moduli must be in [2, 2^62)");
+  if (p.p > p.q4 || p.q4 > p.q3) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "moduli must satisfy p <= q4 <= q3");
+}
+
+u64 lwe_len(const via_params& p) { return (u64)(p.q1_1 ? 2 : 1) * (p.n1 + 1); }
+u64 query_lwes(const via_params& p) {
+  u64 d3 = p.n1 / p.n_rec;
+  return (u64)(ilog2(p.num_rows) + ilog2(p.num_cols) + (d3 > 1 ? ilog2(d3) : 0)) * p.l_query;
+}
+u64 cascade_key_len(const via_params& p) {
+  return (u64)ilog2(p.n1) * 2 * p.n1 * p.l_ck * 2 * (p.q1_1 ? 2 : 1);
+}
+u64 conv_key_len(const via_params& p) { return (u64)p.l_ck * 2 * (p.q1_1 ? 2 : 1) * p.n1; }
+u64 rsk_len(const via_params& p) { return (u64)(p.n1 / p.n2) * p.l_rsk * 2 * p.n2; }
+
+static u64 h_inv(u64 a, u64 m) {
+  i128 t = 0, nt = 1, r = m, nr = a % m;
+  while (nr) {
+    i128 qq = r / nr, tmp = t - qq * nt;
+    t = nt;
+    nt = tmp;
+    tmp = r - qq * nr;
+    r = nr;
+    nr = tmp;
+  }
+  if (r != 1) return 0;
+  return (u64)(t < 0 ? t + m : t);
+}
+
+static DevRing make_ring(Server& s, int n, u64 q0, u64 q1) {
+  DevRing R;
+  R.n = n;
+  R.nl = q1 ? 2 : 1;
+  R.m[0] = make_devmod(q0);
+  if (q1) {
+    R.m[1] = make_devmod(q1);
+    R.q0inv_mod_q1 = h_inv(q0 % q1, q1);
+    if (!R.q0inv_mod_q1) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "q1 RNS primes are not coprime");
+    R.q0inv_shoup = (u64)(((u128)R.q0inv_mod_q1 << 64) / q1);
+  } else {
+    R.m[1] = R.m[0];
+  }
+  // Lazy 128-bit multiply-accumulates need T * q^2 < 2^128 for T <= 256 terms.
+  bool ok = q0 < (1ull << 50) && q1 < (1ull << 50) && is_ntt_friendly(q0, n) && (!q1 || is_ntt_friendly(q1, n));
+  if (ok) {
+    for (int l = 0; l < R.nl; ++l) {
+      u64 q = l ? q1 : q0;
+      // Reuse a table of this prime when one with nmax >= n exists.
+      const NttTable* found = nullptr;
+      for (auto& t : s.tables)
+        if (t.valid && t.dev.q == q && t.dev.nmax >= n) found = &t.dev;
+      if (!found) {
+        int nmax = n;
+        while (nmax < 4096 && is_ntt_friendly(q, nmax * 2)) nmax *= 2;
+        s.tables.push_back(make_ntt_table(q, nmax));
+        found = &s.tables.back().dev;
+      }
+      R.t[l] = *found;
+    }
+    if (R.nl == 1) R.t[1] = R.t[0];
+    R.ntt = true;
+  }
+  return R;
+}
+
+// setup_db (srv/setup_db.rs:39-75) for one record slot k: record k*I*J + r
+// lands in cell r at coefficient positions d*c + k, lifted p -> q2 unchanged.
+__global__ void k_encode_slot(const void* __restrict__ recs, int fmt, u64 count, u64 r0, int k, int n1, int d,
+                              int n_rec, u64 p, u64* __restrict__ db) {
+  u64 gid = (u64)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count * (u64)n_rec) return;
+  u64 r = gid / n_rec;
+  int c = (int)(gid % n_rec);
+  u64 v;
+  if (fmt == VIA_RECORDS_U64) {
+    v = ((const u64*)recs)[gid];
+  } else {
+    unsigned char b = ((const unsigned char*)recs)[gid >> 1];
+    v = (c & 1) ? (b >> 4) : (b & 15);
+  }
+  v = (p & (p - 1)) == 0 ? (v & (p - 1)) : v % p;
+  db[(r0 + r) * (u64)n1 + (u64)d * c + k] = v;
+}
+
+Server::~Server() {
+  workspace_destroy(*this);
+  for (auto& t : tables) free_ntt_table(t);
+  if (stream) cudaStreamDestroy(stream);
+}
+
+static void transform_keys(Server& s) {
+  const via_params& p = s.prm;
+  // Cascade: step k (output degree 2^k) has 2*n1*L_CK*2*nl residues.
+  if (s.r1.ntt) {
+    u64 step = (u64)2 * p.n1 * p.l_ck * 2 * s.r1.nl;
+    for (int k = 1, nout = 2; nout <= (int)p.n1; ++k, nout <<= 1)
+      ntt_forward(s.cascade_eval.p + (k - 1) * step, nout, s.r1.nl, (long)(step / nout), s.r1.t[0], s.r1.t[1],
+                  s.stream);
+    ntt_forward(s.conv_eval.p, p.n1, s.r1.nl, (long)p.l_ck * 2 * s.r1.nl, s.r1.t[0], s.r1.t[1], s.stream);
+  }
+  if (s.r3.ntt)
+    ntt_forward(s.rsk_eval.p, p.n2, 1, (long)(p.n1 / p.n2) * p.l_rsk * 2, s.r3.t[0], s.r3.t[1], s.stream);
+}
+
+static void setup(Server& s, const via_params& p, const via_public_keys* keys, const void* records, u64 n_records,
+                  via_record_format fmt) {
+  validate_params(p);
+  s.prm = p;
+  if (fmt != VIA_RECORDS_U64 && fmt != VIA_RECORDS_NIBBLE) throw ApiError(VIA_ERR_UNKNOWN_FORMAT_TAG, "unknown record format");
+  if (fmt == VIA_RECORDS_NIBBLE && (p.p > 16 || p.n_rec % 2)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "nibble records need p <= 16");
+  u64 I = p.num_rows, J = p.num_cols;
+  int d = (int)(p.n1 / p.n_rec);
+  if (n_records > I * J * (u64)d)
+    throw ApiError(VIA_ERR_DIM_MISMATCH, "setup: more records than DB capacity (would silently drop)");
+  if (n_records && !records) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "records is null");
+  VIA_CUDA(cudaGetDevice(&s.device));
+  VIA_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  s.r1 = make_ring(s, p.n1, p.q1_0, p.q1_1);
+  s.r2 = make_ring(s, p.n1, p.q2, 0);
+  s.r3n1 = make_ring(s, p.n1, p.q3, 0);
+  s.r3 = make_ring(s, p.n2, p.q3, 0);
+  s.r4 = make_ring(s, p.n2, p.q4, 0);
+
+  // Prepared database.
+  s.db.alloc(I * J * p.n1);
+  VIA_CUDA(cudaMemsetAsync(s.db.p, 0, s.db.n * 8, s.stream));
+  size_t rec_bytes = fmt == VIA_RECORDS_U64 ? (size_t)p.n_rec * 8 : (size_t)p.n_rec / 2;
+  const size_t chunk_records = std::max<size_t>(1, ((size_t)256 << 20) / rec_bytes);
+  void* stage = nullptr;
+  if (n_records) VIA_CUDA(cudaMalloc(&stage, std::min<size_t>(chunk_records, I * J) * rec_bytes));
+  try {
+    for (int k = 0; k < d; ++k) {
+      u64 lo = (u64)k * I * J;
+      if (lo >= n_records) break;
+      u64 hi = std::min<u64>(n_records, lo + I * J);
+      for (u64 c0 = lo; c0 < hi; c0 += chunk_records) {
+        u64 c1 = std::min<u64>(hi, c0 + chunk_records);
+        const char* src = (const char*)records + (size_t)c0 * rec_bytes;
+        VIA_CUDA(cudaMemcpyAsync(stage, src, (size_t)(c1 - c0) * rec_bytes, cudaMemcpyHostToDevice, s.stream));
+        u64 threads = (c1 - c0) * p.n_rec;
+        k_encode_slot<<<(unsigned)((threads + 255) / 256), 256, 0, s.stream>>>(stage, fmt, c1 - c0, c0 - lo, k,
+                                                                               p.n1, d, p.n_rec, p.p, s.db.p);
+        VIA_LAUNCHED();
+        VIA_CUDA(cudaStreamSynchronize(s.stream));
+      }
+    }
+  } catch (...) {
+    cudaFree(stage);
+    throw;
+  }
+  if (stage) cudaFree(stage);
+  if (s.r2.ntt) ntt_forward(s.db.p, p.n1, 1, (long)(I * J), s.r2.t[0], s.r2.t[0], s.stream);
+
+  // Keys.
+  if (keys) {
+    if (!keys->cascade_key || !keys->conv_key || !keys->rsk) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null key buffer");
+    s.cascade_eval.alloc(cascade_key_len(p));
+    s.conv_eval.alloc(conv_key_len(p));
+    s.rsk_eval.alloc(rsk_len(p));
+    VIA_CUDA(cudaMemcpyAsync(s.cascade_eval.p, keys->cascade_key, s.cascade_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+    VIA_CUDA(cudaMemcpyAsync(s.conv_eval.p, keys->conv_key, s.conv_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+    VIA_CUDA(cudaMemcpyAsync(s.rsk_eval.p, keys->rsk, s.rsk_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+    transform_keys(s);
+  }
+  workspace_create(s);
+  VIA_CUDA(cudaStreamSynchronize(s.stream));
+}
+
+}  // namespace via
+
+using namespace via;
+
+extern "C" {
+
+const char* via_last_error(void) { return g_last_error.c_str(); }
+
+uint64_t via_lwe_len(const via_params* p) { return p ? lwe_len(*p) : 0; }
+uint64_t via_query_len(const via_params* p) { return p ? query_lwes(*p) : 0; }
+uint64_t via_cascade_key_len(const via_params* p) { return p ? cascade_key_len(*p) : 0; }
+uint64_t via_conv_key_len(const via_params* p) { return p ? conv_key_len(*p) : 0; }
+uint64_t via_rsk_len(const via_params* p) { return p ? rsk_len(*p) : 0; }
+
+via_status via_server_setup(const via_params* params, const via_public_keys* keys, const void* records,
+                            uint64_t n_records, via_record_format format, via_server** out) {
+  return guarded([&] {
+    if (!params || !out) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::unique_ptr<via_server> s(new via_server());
+    setup(*s, *params, keys, records, n_records, format);
+    *out = s.release();
+  });
+}
+
+void via_server_destroy(via_server* s) { delete s; }
+
+via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* out, void* stream) {
+  return guarded([&] {
+    if (!s || !switched || !out) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    cudaStream_t st = (cudaStream_t)stream;
+    const via_params& p = s->prm;
+    DevBuf sel(2 * p.num_rows * p.n1);
+    VIA_CUDA(cudaMemcpyAsync(sel.p, switched, sel.n * 8, cudaMemcpyDeviceToDevice, st));
+    if (s->r2.ntt) ntt_forward(sel.p, p.n1, 1, (long)(2 * p.num_rows), s->r2.t[0], s->r2.t[0], st);
+    first_dim_eval(s->db.p, sel.p, out, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt, st);
+    if (s->r2.ntt) ntt_inverse(out, p.n1, 1, (long)(2 * p.num_cols), s->r2.t[0], s->r2.t[0], st);
+    VIA_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+via_status via_server_answer_dev(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
+                                 uint64_t* out_body, void* stream) {
+  return guarded([&] {
+    if (!s || !query || !out_mask || !out_body) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    u64 expected = query_lwes(s->prm);
+    if (n_lwe != expected)
+      throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " + std::to_string(expected) +
+                                                        " ciphertexts, got " + std::to_string(n_lwe));
+    if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+    std::lock_guard<std::mutex> g(s->mu);
+    answer_device(*s, query, out_mask, out_body, (cudaStream_t)stream);
+  });
+}
+
+via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream) {
+  return guarded([&] {
+    if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    const via_params& p = s->prm;
+    first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
+                   (cudaStream_t)stream);
+  });
+}
+
+via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe, int stage, uint64_t* out,
+                           uint64_t out_len) {
+  return guarded([&] {
+    if (!s || !query || !out) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    if (stage < 1 || stage > 7) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "stage must be in 1..7");
+    const via_params& p = s->prm;
+    if (n_lwe != query_lwes(p)) throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch");
+    u64 nl = p.q1_1 ? 2 : 1, nb = query_lwes(p) / p.l_query;
+    u64 sizes[8] = {0, n_lwe * 2 * nl * p.n1, nb * 2 * p.l_query * 2 * nl * p.n1, p.num_rows * 2 * nl * p.n1,
+                    p.num_rows * 2 * p.n1, p.num_cols * 2 * p.n1, 2 * (u64)p.n1, 2 * (u64)p.n1};
+    if (out_len < sizes[stage]) throw ApiError(VIA_ERR_BUFFER_TOO_SHORT, "debug buffer too short");
+    std::lock_guard<std::mutex> g(s->mu);
+    DevBuf dq(n_lwe * lwe_len(p)), dm(p.n2), db(p.n2), dout(sizes[stage]);
+    VIA_CUDA(cudaMemcpyAsync(dq.p, query, dq.n * 8, cudaMemcpyHostToDevice, s->stream));
+    answer_device_stages(*s, dq.p, dm.p, db.p, s->stream, stage, dout.p);
+    VIA_CUDA(cudaMemcpyAsync(out, dout.p, sizes[stage] * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaStreamSynchronize(s->stream));
+  });
+}
+
+uint64_t via_kernel_launches(void) { return __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED); }
+
+via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
+                             uint64_t* out_body) {
+  return guarded([&] {
+    if (!s || !query || !out_mask || !out_body) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    const via_params& p = s->prm;
+    u64 expected = query_lwes(p);
+    if (n_lwe != expected)
+      throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " + std::to_string(expected) +
+                                                        " ciphertexts, got " + std::to_string(n_lwe));
+    if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+    u64 qlen = n_lwe * lwe_len(p);
+    std::lock_guard<std::mutex> g(s->mu);
+    DevBuf dq(qlen), dm(p.n2), db(p.n2);
+    VIA_CUDA(cudaMemcpyAsync(dq.p, query, qlen * 8, cudaMemcpyHostToDevice, s->stream));
+    answer_device(*s, dq.p, dm.p, db.p, s->stream);
+    VIA_CUDA(cudaMemcpyAsync(out_mask, dm.p, p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaMemcpyAsync(out_body, db.p, p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaStreamSynchronize(s->stream));
+  });
+}
+
+}  // extern "C"

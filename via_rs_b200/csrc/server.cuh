@@ -1,0 +1,80 @@
+// The device-resident server: parameters, NTT tables, prepared database and
+// eval-form keys (crates/via-server/src/{answer,prepared_db,prepared_keys}.rs).
+#pragma once
+#include <memory>
+#include <mutex>
+#include <vector>
+
+#include "../../include/via_gpu.h"
+#include "common.cuh"
+#include "ntt.cuh"
+
+namespace via {
+
+// A ring as the kernels see it: degree, limb count and per-limb modulus/tables.
+struct DevRing {
+  int n = 0;
+  int nl = 1;
+  DevMod m[2];
+  NttTable t[2];  // valid iff ntt
+  bool ntt = false;
+  u64 q0inv_mod_q1 = 0, q0inv_shoup = 0;  // CRT constants when nl == 2
+  __host__ __device__ u128 Q() const { return nl == 1 ? (u128)m[0].q : (u128)m[0].q * m[1].q; }
+  size_t size() const { return (size_t)nl * n; }
+};
+
+// Device buffer with RAII.
+struct DevBuf {
+  u64* p = nullptr;
+  size_t n = 0;
+  DevBuf() = default;
+  explicit DevBuf(size_t count) { alloc(count); }
+  void alloc(size_t count);
+  void free();
+  ~DevBuf() { free(); }
+  DevBuf(const DevBuf&) = delete;
+  DevBuf& operator=(const DevBuf&) = delete;
+};
+
+struct Workspace;  // per-query scratch (pipeline.cu)
+struct WorkspaceDeleter {
+  void operator()(Workspace* w) const;
+};
+
+struct Server {
+  via_params prm{};
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  // Rings: q1 at n1 (1 or 2 limbs), q2 at n1, q3 at n1 and n2, q4 at n2.
+  DevRing r1, r2, r3n1, r3, r4;
+  std::vector<NttTableHost> tables;  // owners
+  // Prepared database: [I][J][n1] eval-form residues mod q2.
+  DevBuf db;
+  // Eval-form keys (crates/via-server/src/prepared_keys.rs:69-79).
+  DevBuf cascade_eval;  // include/via_gpu.h cascade layout, each segment transformed
+  DevBuf conv_eval;     // L_CK samples at (q1, n1)
+  DevBuf rsk_eval;      // d RLevs at (q3, n2)
+  std::unique_ptr<Workspace, WorkspaceDeleter> ws;
+  std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
+  ~Server();
+};
+
+// Shared helpers.
+void validate_params(const via_params& p);
+u64 lwe_len(const via_params& p);
+u64 query_lwes(const via_params& p);
+u64 cascade_key_len(const via_params& p);
+u64 conv_key_len(const via_params& p);
+u64 rsk_len(const via_params& p);
+int ilog2(u64 v);
+
+// Pipeline entry points (pipeline.cu).
+void workspace_create(Server& s);
+void workspace_destroy(Server& s);
+void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st);
+void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st, int stop_stage,
+                          u64* dump);
+
+}  // namespace via
+
+struct via_server : via::Server {};

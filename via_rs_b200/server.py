@@ -1,0 +1,152 @@
+"""Host-side mirror of via-server's `Server` (crates/via-server/src/answer.rs:423-603).
+
+    server = Server.setup(params, keys, records)     # Server::setup
+    mask, body = server.answer(query)                 # Server::answer
+
+Errors mirror `via_protocol::ViaError` (crates/via-protocol/src/error.rs:20-64):
+the reference returns `Err(ViaError::DimMismatch(..))` /
+`Err(ViaError::QueryLengthMismatch{..})`; here the same conditions raise
+`DimMismatch` / `QueryLengthMismatch`.
+"""
+import ctypes
+
+import numpy as np
+
+from . import _lib
+from .params import Params
+
+VIA_RECORDS_U64 = 0
+VIA_RECORDS_NIBBLE = 1
+
+
+class ViaError(RuntimeError):
+    code = -1
+
+
+class SetupNotComplete(ViaError):
+    code = 1
+
+
+class IndexOutOfRange(ViaError):
+    code = 2
+
+
+class QueryLengthMismatch(ViaError):
+    code = 3
+
+
+class BufferTooShort(ViaError):
+    code = 4
+
+
+class UnknownFormatTag(ViaError):
+    code = 5
+
+
+class DimMismatch(ViaError):
+    code = 7
+
+
+class DeviceError(ViaError):
+    """A device-side failure (allocation, CUDA call, bounded wait)."""
+
+
+_BY_CODE = {c.code: c for c in (SetupNotComplete, IndexOutOfRange, QueryLengthMismatch, BufferTooShort,
+                               UnknownFormatTag, DimMismatch)}
+
+
+def check(rc: int) -> None:
+    if rc != 0:
+        msg = _lib.lib().via_last_error().decode()
+        cls = _BY_CODE.get(rc, DeviceError)
+        err = cls(f"[{rc}] {msg}")
+        err.code = rc
+        raise err
+
+
+def _u64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(ctypes.POINTER(ctypes.c_uint64))
+
+
+class PublicKeys:
+    """The client's public keys in include/via_gpu.h wire layout."""
+
+    def __init__(self, cascade_key, conv_key, rsk):
+        self.cascade_key = _u64(cascade_key)
+        self.conv_key = _u64(conv_key)
+        self.rsk = _u64(rsk)
+
+
+class Server:
+    def __init__(self, handle, prm: Params):
+        self._h = handle
+        self.prm = prm
+
+    @classmethod
+    def setup(cls, prm: Params, keys: PublicKeys, records, fmt: int = VIA_RECORDS_U64) -> "Server":
+        """Server::setup: encode + prepare the database on the device, upload keys.
+
+        records: for VIA_RECORDS_U64 an array of n_records*n_rec coefficients;
+        for VIA_RECORDS_NIBBLE a uint8 array of n_records*n_rec/2 bytes.
+        """
+        L = _lib.lib()
+        cp = prm.to_c()
+        if len(keys.cascade_key) != prm.cascade_key_len or len(keys.conv_key) != prm.conv_key_len or \
+                len(keys.rsk) != prm.rsk_len:
+            raise BufferTooShort("public key buffers do not match the parameter set")
+        k = _lib.ViaPublicKeys(_ptr(keys.cascade_key), _ptr(keys.conv_key), _ptr(keys.rsk))
+        if fmt == VIA_RECORDS_U64:
+            rec = _u64(records)
+            n = rec.size // prm.n_rec
+        else:
+            rec = np.ascontiguousarray(records, dtype=np.uint8)
+            n = rec.size * 2 // prm.n_rec
+        h = ctypes.c_void_p()
+        check(L.via_server_setup(ctypes.byref(cp), ctypes.byref(k), rec.ctypes.data_as(ctypes.c_void_p), n, fmt,
+                                 ctypes.byref(h)))
+        s = cls(h, prm)
+        s._keys = keys
+        return s
+
+    def answer(self, query):
+        """Server::answer: returns (mask mod q3, body mod q4), n2 residues each."""
+        q = _u64(query)
+        n_lwe = q.size // self.prm.lwe_len
+        if n_lwe * self.prm.lwe_len != q.size:
+            raise BufferTooShort("query buffer is not a whole number of LWEs")
+        mask = np.zeros(self.prm.n2, dtype=np.uint64)
+        body = np.zeros(self.prm.n2, dtype=np.uint64)
+        check(_lib.lib().via_server_answer(self._h, _ptr(q), n_lwe, _ptr(mask), _ptr(body)))
+        return mask, body
+
+    def debug_stage(self, query, stage: int) -> np.ndarray:
+        """The answer's intermediate `stage` (1..7), see via_debug_stage in include/via_gpu.h."""
+        prm = self.prm
+        q = _u64(query)
+        nbits = prm.n_lwe // prm.l_query
+        size = {1: prm.n_lwe * 2 * prm.nl * prm.n1, 2: nbits * 2 * prm.l_query * 2 * prm.nl * prm.n1,
+                3: prm.num_rows * 2 * prm.nl * prm.n1, 4: prm.num_rows * 2 * prm.n1, 5: prm.num_cols * 2 * prm.n1,
+                6: 2 * prm.n1, 7: 2 * prm.n1}[stage]
+        out = np.zeros(size, dtype=np.uint64)
+        check(_lib.lib().via_debug_stage(self._h, _ptr(q), q.size // prm.lwe_len, stage, _ptr(out), size))
+        return out
+
+    def first_dim_dev(self, switched_ptr: int, out_ptr: int, stream: int = 0) -> None:
+        """FirstDim on device buffers (I RLWEs at q2 in, J RLWEs out)."""
+        check(_lib.lib().via_first_dim_dev(self._h, ctypes.c_void_p(switched_ptr), ctypes.c_void_p(out_ptr),
+                                           ctypes.c_void_p(stream)))
+
+    def close(self) -> None:
+        if self._h:
+            _lib.lib().via_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
