@@ -422,7 +422,7 @@ static void mac(const DevRing& R, const u64* D, const u64* K, u64* out, int T, i
 
 static void decompose(const DevRing& R, const Gadget& g, const u64* in, int n_in, int stride, long npolys, u64* out,
                       cudaStream_t st) {
-  k_decompose<<<blocks(npolys * n_in), 128, 0, st>>>(in, n_in, stride, npolys, R, g, out);
+  k_decompose<<<blocks(npolys * n_in, 128), 128, 0, st>>>(in, n_in, stride, npolys, R, g, out);
   VIA_LAUNCHED();
 }
 
