@@ -3,42 +3,82 @@
 //   c_j = sum_i sel_i (.) db[i][j]   for every column j, mask and body,
 //
 // computed pointwise in the eval domain at q2. The database is HBM-resident in
-// eval form, one u64 per residue, laid out [i][j][t] (t = eval slot), so that a
-// warp reads 512 contiguous bytes per (i, j) and each thread streams its column
-// group with 16-byte loads. Products are summed exactly in 128 bits and reduced
-// once per output residue (sum < I * q2^2 < 2^128).
+// eval form, one u64 per residue, laid out [i][j][t] (t = eval slot): a warp
+// reads 512 contiguous bytes per (i, j) and each thread streams its columns with
+// 16-byte loads.
+//
+// Exact products without 128-bit arithmetic: every selection residue s < q2 <
+// 2^34 is split once per query into s = s0 + 2^17 s1 (s0, s1 < 2^17), and every
+// database residue d < 2^34 is read as d = dl + 2^32 dh (dh < 4). Then
+//   sum_i d s = A0 + 2^32 H0 + 2^17 (A1 + 2^32 H1),
+//   A_k = sum dl s_k  (< I 2^49, a 64-bit IMAD.WIDE accumulator),
+//   H_k = sum dh s_k  (< I 2^19, a 32-bit IMAD accumulator),
+// exact for I <= 4096, reduced mod q2 once per output residue.
 #include "first_dim.cuh"
 
 namespace via {
 
-constexpr int FD_TPT = 2;  // eval slots per thread (one 16-byte load)
+constexpr int FD_TPT = 2;  // eval slots per thread (one 16-byte load per column)
 constexpr int FD_THREADS = 128;
 
+// sel (I RLWEs, [I][2][n] u64 < 2^34) -> split halves [I][2][n] as (s0, s1).
+__global__ void k_split_sel(const u64* __restrict__ sel, uint2* __restrict__ out, long count) {
+  long g = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (g >= count) return;
+  u64 s = sel[g];
+  out[g] = make_uint2((u32)(s & 0x1FFFF), (u32)(s >> 17));
+}
+
+struct SplitAcc {
+  u64 a0, a1;
+  u32 h0, h1;
+};
+
+__device__ __forceinline__ void split_mac(SplitAcc& acc, u64 d, uint2 s) {
+  const u32 dl = (u32)d, dh = (u32)(d >> 32);
+  acc.a0 += (u64)dl * s.x;  // IMAD.WIDE.U32
+  acc.a1 += (u64)dl * s.y;
+  acc.h0 += dh * s.x;       // IMAD
+  acc.h1 += dh * s.y;
+}
+
+__device__ __forceinline__ u64 split_reduce(const SplitAcc& a, const DevMod& m) {
+  u64 x0 = a.a0 + ((u64)a.h0 << 32);
+  u64 x1 = a.a1 + ((u64)a.h1 << 32);
+  // x0 + 2^17 x1 as 128 bits.
+  u64 lo = x0 + (x1 << 17);
+  u64 hi = (x1 >> 47) + (lo < x0 ? 1 : 0);
+  return reduce128(hi, lo, m);
+}
+
 template <int JPT>
-__global__ void __launch_bounds__(FD_THREADS) k_first_dim_ntt(const u64* __restrict__ db, const u64* __restrict__ sel,
+__global__ void __launch_bounds__(FD_THREADS) k_first_dim_ntt(const u64* __restrict__ db, const uint2* __restrict__ sel,
                                                               u64* __restrict__ out, int I, int J, int n, DevMod m) {
   const int t = (blockIdx.x * FD_THREADS + threadIdx.x) * FD_TPT;
   const int j0 = blockIdx.y * JPT;
   if (t >= n) return;
-  Acc128 am[JPT][FD_TPT], ab[JPT][FD_TPT];
+  SplitAcc am[JPT][FD_TPT], ab[JPT][FD_TPT];
 #pragma unroll
   for (int jj = 0; jj < JPT; ++jj)
 #pragma unroll
-    for (int k = 0; k < FD_TPT; ++k) am[jj][k] = ab[jj][k] = Acc128{0, 0};
+    for (int k = 0; k < FD_TPT; ++k) am[jj][k] = ab[jj][k] = SplitAcc{0, 0, 0, 0};
   const size_t row_stride = (size_t)J * n;
   const u64* dbp = db + (size_t)j0 * n + t;
+  const uint4* selp = reinterpret_cast<const uint4*>(sel + t);
+  const size_t sel_stride = (size_t)n / 2;  // uint4 per poly (2 slots per uint4)
+#pragma unroll 2
   for (int i = 0; i < I; ++i) {
-    const ulonglong2 sm = *reinterpret_cast<const ulonglong2*>(sel + (size_t)(2 * i) * n + t);
-    const ulonglong2 sb = *reinterpret_cast<const ulonglong2*>(sel + (size_t)(2 * i + 1) * n + t);
+    const uint4 sm = __ldg(selp + (size_t)(2 * i) * sel_stride);
+    const uint4 sb = __ldg(selp + (size_t)(2 * i + 1) * sel_stride);
     ulonglong2 d[JPT];
 #pragma unroll
     for (int jj = 0; jj < JPT; ++jj) d[jj] = __ldcs(reinterpret_cast<const ulonglong2*>(dbp + (size_t)jj * n));
 #pragma unroll
     for (int jj = 0; jj < JPT; ++jj) {
-      mac128(am[jj][0], d[jj].x, sm.x);
-      mac128(am[jj][1], d[jj].y, sm.y);
-      mac128(ab[jj][0], d[jj].x, sb.x);
-      mac128(ab[jj][1], d[jj].y, sb.y);
+      split_mac(am[jj][0], d[jj].x, make_uint2(sm.x, sm.y));
+      split_mac(am[jj][1], d[jj].y, make_uint2(sm.z, sm.w));
+      split_mac(ab[jj][0], d[jj].x, make_uint2(sb.x, sb.y));
+      split_mac(ab[jj][1], d[jj].y, make_uint2(sb.z, sb.w));
     }
     dbp += row_stride;
   }
@@ -46,10 +86,10 @@ __global__ void __launch_bounds__(FD_THREADS) k_first_dim_ntt(const u64* __restr
   for (int jj = 0; jj < JPT; ++jj) {
     u64* o = out + (size_t)(2 * (j0 + jj)) * n + t;
     ulonglong2 rm, rb;
-    rm.x = reduce128(am[jj][0].hi, am[jj][0].lo, m);
-    rm.y = reduce128(am[jj][1].hi, am[jj][1].lo, m);
-    rb.x = reduce128(ab[jj][0].hi, ab[jj][0].lo, m);
-    rb.y = reduce128(ab[jj][1].hi, ab[jj][1].lo, m);
+    rm.x = split_reduce(am[jj][0], m);
+    rm.y = split_reduce(am[jj][1], m);
+    rb.x = split_reduce(ab[jj][0], m);
+    rb.y = split_reduce(ab[jj][1], m);
     *reinterpret_cast<ulonglong2*>(o) = rm;
     *reinterpret_cast<ulonglong2*>(o + n) = rb;
   }
@@ -100,21 +140,31 @@ __global__ void k_first_dim_schoolbook(const u64* __restrict__ db, const u64* __
   out[(size_t)(2 * j + 1) * n + t] = rb;
 }
 
-void first_dim_eval(const u64* db, const u64* sel_eval, u64* out_eval, int I, int J, int n, const DevMod& m,
-                    bool ntt, cudaStream_t st) {
-  if (ntt) {
-    constexpr int JPT = 8;
-    if (J % JPT != 0 || n % (FD_THREADS * FD_TPT) != 0) {
-      // Small shapes: one column per thread group.
-      dim3 grid((n + FD_THREADS * FD_TPT - 1) / (FD_THREADS * FD_TPT), J);
-      k_first_dim_ntt<1><<<grid, FD_THREADS, 0, st>>>(db, sel_eval, out_eval, I, J, n, m);
-    } else {
-      dim3 grid(n / (FD_THREADS * FD_TPT), J / JPT);
-      k_first_dim_ntt<JPT><<<grid, FD_THREADS, 0, st>>>(db, sel_eval, out_eval, I, J, n, m);
+int first_dim_variants() { return 3; }
+static int jpt_of(int v) { return v == 0 ? 2 : (v == 1 ? 4 : 8); }
+
+bool first_dim_split_ok(int I, int n, u64 q) { return I <= 4096 && q < (1ull << 34) && n % 2 == 0; }
+
+void first_dim_eval(const u64* db, const u64* sel_eval, u64* out_eval, int I, int J, int n, const DevMod& m, bool ntt,
+                    cudaStream_t st, uint2* sel_split, int variant) {
+  if (ntt && sel_split && first_dim_split_ok(I, n, m.q)) {
+    long cnt = (long)I * 2 * n;
+    k_split_sel<<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(sel_eval, sel_split, cnt);
+    VIA_LAUNCHED();
+    int jpt = jpt_of(variant);
+    while (J % jpt) jpt >>= 1;
+    dim3 grid((n + FD_THREADS * FD_TPT - 1) / (FD_THREADS * FD_TPT), J / jpt);
+    switch (jpt) {
+      case 8: k_first_dim_ntt<8><<<grid, FD_THREADS, 0, st>>>(db, sel_split, out_eval, I, J, n, m); break;
+      case 4: k_first_dim_ntt<4><<<grid, FD_THREADS, 0, st>>>(db, sel_split, out_eval, I, J, n, m); break;
+      case 2: k_first_dim_ntt<2><<<grid, FD_THREADS, 0, st>>>(db, sel_split, out_eval, I, J, n, m); break;
+      default: k_first_dim_ntt<1><<<grid, FD_THREADS, 0, st>>>(db, sel_split, out_eval, I, J, n, m); break;
     }
-  } else {
+  } else if (!ntt) {
     long total = (long)J * n;
     k_first_dim_schoolbook<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(db, sel_eval, out_eval, I, J, n, m);
+  } else {
+    throw CudaError(100, "first_dim: shape outside the split-accumulator bounds (I <= 4096, q2 < 2^34)");
   }
   VIA_LAUNCHED();
 }

@@ -99,58 +99,158 @@ void free_ntt_table(NttTableHost& t) {
 
 constexpr int NTT_THREADS = 256;
 
-// One CTA transforms a tile of `tile` coefficients (tile/n whole segments).
-template <bool INV>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt(u64* __restrict__ data, int logn, int nl, long segments,
-                                                     int tile, NttTable t0, NttTable t1) {
-  extern __shared__ u64 sm[];
-  const int n = 1 << logn;
-  const int spt = tile >> logn;  // segments per tile
-  const long seg0 = (long)blockIdx.x * spt;
-  const int nseg = (int)min((long)spt, segments - seg0);
-  const int count = nseg << logn;
-  u64* g = data + (seg0 << logn);
-  for (int i = threadIdx.x; i < count; i += NTT_THREADS) sm[i] = g[i];
-  __syncthreads();
-  const int half = n >> 1;
-  const int nbf = count >> 1;  // butterflies per stage
-  if (!INV) {
-    for (int len = half, m = 1; len >= 1; len >>= 1, m <<= 1) {
-      for (int b = threadIdx.x; b < nbf; b += NTT_THREADS) {
-        int sl = b >> (logn - 1), bb = b & (half - 1);
-        int grp = bb / len, j = bb - grp * len;
-        int i0 = (sl << logn) + grp * 2 * len + j, i1 = i0 + len;
-        const NttTable& T = (nl == 2 && ((seg0 + sl) & 1)) ? t1 : t0;
-        u64 q = T.q;
-        u64 u = sm[i0];
-        u64 v = mul_shoup(sm[i1], T.psi[m + grp], T.psi_sh[m + grp], q);
-        sm[i0] = addmod(u, v, q);
-        sm[i1] = submod(u, v, q);
+// ---------------------------------------------------------------------------
+// Register-resident transform for n >= 8: every thread holds 8 residues and
+// performs up to three butterfly stages (a radix-8 step) on them before the
+// residues are exchanged through shared memory. A CTA of 256 threads handles
+// 2048/n segments (one segment = one limb of one polynomial).
+//
+// Stage s of the forward transform pairs (x, x + len_s), len_s = n >> (s+1),
+// twiddle psi[n/(2 len_s) + x/(2 len_s)] (Cooley-Tukey on bit-reversed twiddles);
+// the inverse runs len = 1, 2, ..., n/2 with Gentleman-Sande butterflies and
+// psi^-1, then scales by n^-1. A phase of r stages works on sub-blocks of 2^r
+// residues x = base + k*stride, k < 2^r, where stride is the phase's smallest
+// len and base = (u / stride) * (stride << r) + u % stride over the n >> r
+// sub-blocks u; a thread owns 8 >> r consecutive sub-blocks.
+// ---------------------------------------------------------------------------
+template <int LOGN, bool INV, int P>
+struct NttPhase {
+  static constexpr int n = 1 << LOGN;
+  static constexpr int S0 = 3 * P;
+  static constexpr int R = (LOGN - S0) < 3 ? (LOGN - S0) : 3;
+  static constexpr int NSUB = 8 >> R;
+  // Smallest stage len of the phase (see k_ntt_reg).
+  static constexpr int STRIDE = INV ? (1 << S0) : ((n >> (S0 + 1)) >> (R - 1));
+
+  __device__ __forceinline__ static int index(int v, int tid) {
+    const int sub = v >> R, k = v & ((1 << R) - 1);
+    const int u = tid * NSUB + sub;
+    return (u / STRIDE) * (STRIDE << R) + (u % STRIDE) + k * STRIDE;
+  }
+
+  __device__ __forceinline__ static void run(u64 (&e)[8], int tid, const NttTable& T) {
+    const u64 q = T.q;
+#pragma unroll
+    for (int sub = 0; sub < NSUB; ++sub) {
+      const int u = tid * NSUB + sub;
+      const int base = (u / STRIDE) * (STRIDE << R) + (u % STRIDE);
+#pragma unroll
+      for (int lvl = 0; lvl < R; ++lvl) {
+        // forward: len = STRIDE << (R-1-lvl) (decreasing); inverse: STRIDE << lvl.
+        const int hk = INV ? (1 << lvl) : (1 << (R - 1 - lvl));
+        const int len = STRIDE * hk;
+        const int m = n / (2 * len);
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+          if (k & hk) continue;
+          const int x = base + k * STRIDE;
+          const int grp = x / (2 * len);
+          u64& a = e[sub * (1 << R) + k];
+          u64& c = e[sub * (1 << R) + k + hk];
+          if (!INV) {
+            const u64 w = __ldg(T.psi + m + grp), ws = __ldg(T.psi_sh + m + grp);
+            const u64 t = mul_shoup(c, w, ws, q);
+            const u64 av = a;
+            a = addmod(av, t, q);
+            c = submod(av, t, q);
+          } else {
+            const u64 w = __ldg(T.ipsi + m + grp), ws = __ldg(T.ipsi_sh + m + grp);
+            const u64 av = a, cv = c;
+            a = addmod(av, cv, q);
+            c = mul_shoup(submod(av, cv, q), w, ws, q);
+          }
+        }
       }
-      __syncthreads();
+    }
+  }
+};
+
+template <int LOGN, bool INV, int P>
+__device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* ssm, bool active) {
+  using Ph = NttPhase<LOGN, INV, P>;
+  constexpr int NPH = (LOGN + 2) / 3;
+  if (P == 0) {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = active ? g[Ph::index(v, tid)] : 0;
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = ssm[Ph::index(v, tid)];
+  }
+  Ph::run(e, tid, T);
+  if constexpr (P == NPH - 1) {
+    if (INV) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q);
+    }
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) g[Ph::index(v, tid)] = e[v];
     }
   } else {
-    for (int len = 1, m = half; len < n; len <<= 1, m >>= 1) {
-      for (int b = threadIdx.x; b < nbf; b += NTT_THREADS) {
-        int sl = b >> (logn - 1), bb = b & (half - 1);
-        int grp = bb / len, j = bb - grp * len;
-        int i0 = (sl << logn) + grp * 2 * len + j, i1 = i0 + len;
-        const NttTable& T = (nl == 2 && ((seg0 + sl) & 1)) ? t1 : t0;
-        u64 q = T.q;
-        u64 u = sm[i0], v = sm[i1];
-        sm[i0] = addmod(u, v, q);
-        sm[i1] = mul_shoup(submod(u, v, q), T.ipsi[m + grp], T.ipsi_sh[m + grp], q);
-      }
-      __syncthreads();
-    }
-    for (int i = threadIdx.x; i < count; i += NTT_THREADS) {
-      int sl = i >> logn;
-      const NttTable& T = (nl == 2 && ((seg0 + sl) & 1)) ? t1 : t0;
-      sm[i] = mul_shoup(sm[i], T.ninv[logn], T.ninv_sh[logn], T.q);
-    }
     __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
+    ntt_phases<LOGN, INV, P + 1>(e, tid, T, g, ssm, active);
   }
-  for (int i = threadIdx.x; i < count; i += NTT_THREADS) g[i] = sm[i];
+}
+
+template <int LOGN, bool INV>
+__global__ void __launch_bounds__(NTT_THREADS) k_ntt_reg(u64* __restrict__ data, int nl, long segments, NttTable t0,
+                                                         NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  constexpr int TPS = n / 8;              // threads per segment
+  constexpr int SPC = NTT_THREADS / TPS;  // segments per CTA
+  __shared__ u64 sm[NTT_THREADS * 8];
+  const int seg_local = threadIdx.x / TPS;
+  const int tid = threadIdx.x % TPS;
+  const long seg = (long)blockIdx.x * SPC + seg_local;
+  const bool active = seg < segments;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  u64 e[8];
+  ntt_phases<LOGN, INV, 0>(e, tid, T, data + seg * n, sm + seg_local * n, active);
+}
+
+// n = 2 and 4: one thread per segment, all in registers.
+template <int LOGN, bool INV>
+__global__ void k_ntt_tiny(u64* __restrict__ data, int nl, long segments, NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  long seg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  const u64 q = T.q;
+  u64 a[n];
+  u64* g = data + seg * n;
+#pragma unroll
+  for (int i = 0; i < n; ++i) a[i] = g[i];
+  if (!INV) {
+#pragma unroll
+    for (int len = n / 2, m = 1; len >= 1; len >>= 1, m <<= 1)
+#pragma unroll
+      for (int x = 0; x < n; ++x) {
+        if ((x / len) & 1) continue;
+        const int grp = x / (2 * len);
+        const u64 t = mul_shoup(a[x + len], T.psi[m + grp], T.psi_sh[m + grp], q);
+        const u64 u = a[x];
+        a[x] = addmod(u, t, q);
+        a[x + len] = submod(u, t, q);
+      }
+  } else {
+#pragma unroll
+    for (int len = 1, m = n / 2; len < n; len <<= 1, m >>= 1)
+#pragma unroll
+      for (int x = 0; x < n; ++x) {
+        if ((x / len) & 1) continue;
+        const int grp = x / (2 * len);
+        const u64 u = a[x], c = a[x + len];
+        a[x] = addmod(u, c, q);
+        a[x + len] = mul_shoup(submod(u, c, q), T.ipsi[m + grp], T.ipsi_sh[m + grp], q);
+      }
+#pragma unroll
+    for (int i = 0; i < n; ++i) a[i] = mul_shoup(a[i], T.ninv[LOGN], T.ninv_sh[LOGN], q);
+  }
+#pragma unroll
+  for (int i = 0; i < n; ++i) g[i] = a[i];
 }
 
 template <bool INV>
@@ -158,13 +258,30 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
                    cudaStream_t st) {
   if (segments <= 0) return;
   int logn = __builtin_ctz((unsigned)n);
-  if (n < 2 || (n & (n - 1)) || logn > NTT_MAX_LOGN) throw CudaError(100, "ntt: bad degree");
-  int tile = n > 2048 ? n : 2048;
-  long spt = tile / n;
-  long blocks = (segments + spt - 1) / spt;
-  size_t smem = (size_t)tile * 8;
-  if (smem > 48 * 1024) VIA_CUDA(cudaFuncSetAttribute(k_ntt<INV>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  k_ntt<INV><<<(unsigned)blocks, NTT_THREADS, smem, st>>>(data, logn, nl, segments, tile, t0, t1);
+  if (n < 2 || (n & (n - 1)) || logn > 11) throw CudaError(100, "ntt: degree must be a power of two in [2, 2048]");
+  if (logn <= 2) {
+    unsigned blocks = (unsigned)((segments + 127) / 128);
+    if (logn == 1) k_ntt_tiny<1, INV><<<blocks, 128, 0, st>>>(data, nl, segments, t0, t1);
+    else k_ntt_tiny<2, INV><<<blocks, 128, 0, st>>>(data, nl, segments, t0, t1);
+    VIA_LAUNCHED();
+    return;
+  }
+  long spc = NTT_THREADS / (n / 8);
+  unsigned blocks = (unsigned)((segments + spc - 1) / spc);
+  switch (logn) {
+#define VIA_NTT_CASE(LG) \
+  case LG: k_ntt_reg<LG, INV><<<blocks, NTT_THREADS, 0, st>>>(data, nl, segments, t0, t1); break;
+    VIA_NTT_CASE(3)
+    VIA_NTT_CASE(4)
+    VIA_NTT_CASE(5)
+    VIA_NTT_CASE(6)
+    VIA_NTT_CASE(7)
+    VIA_NTT_CASE(8)
+    VIA_NTT_CASE(9)
+    VIA_NTT_CASE(10)
+    VIA_NTT_CASE(11)
+#undef VIA_NTT_CASE
+  }
   VIA_LAUNCHED();
 }
 

@@ -345,7 +345,7 @@ struct Workspace {
   // DMux.
   DevBuf dm_a, dm_b, dm_digits, dm_ext;
   // FirstDim / CMux.
-  DevBuf sel, fd_out, cm_diff, cm_digits, cm_ext, cm_b;
+  DevBuf sel, sel_split, fd_out, cm_diff, cm_digits, cm_ext, cm_b;
   // CRot / RespComp.
   DevBuf cr_ct, cr_diff, cr_digits, cr_ext, rs_ct3, rs_mproj, rs_bproj, rs_digits, rs_gp, rs_acc;
   Gadget g_ck, g_dmux, g_cmux, g_rsk;
@@ -353,6 +353,37 @@ struct Workspace {
 
 void WorkspaceDeleter::operator()(Workspace* w) const { delete w; }
 void workspace_destroy(Server& s) { s.ws.reset(); }
+uint2* workspace_sel_split(Server& s) { return reinterpret_cast<uint2*>(s.ws->sel_split.p); }
+
+// Times each FirstDim column tile on the prepared database and keeps the fastest.
+void autotune_first_dim(Server& s) {
+  const via_params& p = s.prm;
+  if (!s.r2.ntt || !first_dim_split_ok((int)p.num_rows, (int)p.n1, p.q2)) return;
+  Workspace& w = *s.ws;
+  VIA_CUDA(cudaMemsetAsync(w.sel.p, 0, w.sel.n * 8, s.stream));
+  cudaEvent_t e0, e1;
+  VIA_CUDA(cudaEventCreate(&e0));
+  VIA_CUDA(cudaEventCreate(&e1));
+  float best = 1e30f;
+  for (int v = 0; v < first_dim_variants(); ++v) {
+    first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], true, s.stream,
+                   workspace_sel_split(s), v);
+    VIA_CUDA(cudaEventRecord(e0, s.stream));
+    for (int r = 0; r < 2; ++r)
+      first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], true,
+                     s.stream, workspace_sel_split(s), v);
+    VIA_CUDA(cudaEventRecord(e1, s.stream));
+    VIA_CUDA(cudaEventSynchronize(e1));
+    float ms = 0;
+    VIA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+    if (ms < best) {
+      best = ms;
+      s.fd_variant = v;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+}
 
 void workspace_create(Server& s) {
   const via_params& p = s.prm;
@@ -378,6 +409,7 @@ void workspace_create(Server& s) {
   w->dm_digits.alloc(std::max(1L, I / 2) * 2 * L * nl * n1);
   w->dm_ext.alloc(std::max(1L, I / 2) * 2 * nl * n1);
   w->sel.alloc(I * 2 * n1);
+  w->sel_split.alloc(I * 2 * n1);  // uint2 per residue
   w->fd_out.alloc(J * 2 * n1);
   w->cm_diff.alloc(std::max(1L, J / 2) * 2 * n1);
   w->cm_digits.alloc(std::max(1L, J / 2) * 2 * L * n1);
@@ -544,7 +576,8 @@ void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_bod
 
   // ---- Step 4: FirstDim (answer.rs:204-205) — result stays in the eval domain.
   to_eval(s.r2, w.sel.p, n1, 2 * I, st);
-  first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st);
+  first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st, workspace_sel_split(s),
+                 s.fd_variant);
   if (stop_stage == 5) {
     copy_out(w.fd_out.p, (size_t)J * 2 * n1);
     from_eval(s.r2, dump, n1, 2 * J, st);

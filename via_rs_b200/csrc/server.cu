@@ -235,6 +235,7 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     transform_keys(s);
   }
   workspace_create(s);
+  autotune_first_dim(s);
   VIA_CUDA(cudaStreamSynchronize(s.stream));
 }
 
@@ -273,7 +274,9 @@ via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* 
     DevBuf sel(2 * p.num_rows * p.n1);
     VIA_CUDA(cudaMemcpyAsync(sel.p, switched, sel.n * 8, cudaMemcpyDeviceToDevice, st));
     if (s->r2.ntt) ntt_forward(sel.p, p.n1, 1, (long)(2 * p.num_rows), s->r2.t[0], s->r2.t[0], st);
-    first_dim_eval(s->db.p, sel.p, out, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt, st);
+    std::lock_guard<std::mutex> g(s->mu);
+    first_dim_eval(s->db.p, sel.p, out, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt, st,
+                   workspace_sel_split(*s), s->fd_variant);
     if (s->r2.ntt) ntt_inverse(out, p.n1, 1, (long)(2 * p.num_cols), s->r2.t[0], s->r2.t[0], st);
     VIA_CUDA(cudaStreamSynchronize(st));
   });
@@ -297,8 +300,9 @@ via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint6
   return guarded([&] {
     if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
     const via_params& p = s->prm;
+    std::lock_guard<std::mutex> g(s->mu);
     first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
-                   (cudaStream_t)stream);
+                   (cudaStream_t)stream, workspace_sel_split(*s), s->fd_variant);
   });
 }
 

@@ -56,6 +56,7 @@ struct Server {
   DevBuf rsk_eval;      // d RLevs at (q3, n2)
   std::unique_ptr<Workspace, WorkspaceDeleter> ws;
   std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
+  int fd_variant = 1;  // FirstDim column tile chosen at setup (autotuned)
   ~Server();
 };
 
@@ -71,6 +72,8 @@ int ilog2(u64 v);
 // Pipeline entry points (pipeline.cu).
 void workspace_create(Server& s);
 void workspace_destroy(Server& s);
+uint2* workspace_sel_split(Server& s);
+void autotune_first_dim(Server& s);
 void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st);
 void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st, int stop_stage,
                           u64* dump);
