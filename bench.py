@@ -32,9 +32,11 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "answers/s and DB GB/s scanned, batched vs plain, 1 GiB DB; p50/p99 answer ms"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_first_dim_ntt launch,
-# scaled to the 1 GiB workload (see profiles/first_dim_scan.md); None until captured.
-SCAN_TRAFFIC_BYTES = None
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_first_dim_ntt launch on
+# the I=256, J=256 case (1.082155 GB + 5.650176 MB), scaled by the 16x more
+# database cells of the I=256, J=4096 workload (profiles/first_dim_scan.md).
+SCAN_TRAFFIC_BYTES_SMALL = 1.082155e9 + 5.650176e6
+SCAN_TRAFFIC_CELLS_SMALL = 256 * 256
 
 
 def parse():
@@ -47,6 +49,7 @@ def parse():
     ap.add_argument("--cols", type=int, default=4096)
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU oracle leg (for profiling)")
     ap.add_argument("--scan-launches", type=int, default=10)
+    ap.add_argument("--batch", type=int, default=64, help="queries per shared-scan batch (0 = skip)")
     return ap.parse_args()
 
 
@@ -179,11 +182,13 @@ def reference_arm(args, prm):
 
 
 def config_dict(prm):
-    return {"workload": f"paper VIA-C answer, 1 GiB DB (I={prm.num_rows}, J={prm.num_cols}, n1={prm.n1}), "
+    gib = prm.capacity * prm.n_rec // 2 / (1 << 30)
+    return {"workload": f"paper VIA-C answer, {gib:g} GiB DB (I={prm.num_rows}, J={prm.num_cols}, n1={prm.n1}), "
                         "one query per step",
             "preset": "paper (q1=137438822401*274810798081, q2=17175674881, q3=8380417, q4=4096, p=16)",
             "db_raw_bytes": prm.capacity * prm.n_rec // 2, "db_prepared_bytes": prm.num_rows * prm.num_cols * prm.n1 * 8,
-            "l2": "inputs larger than L2: the 16 GiB prepared DB is streamed every step"}
+            "l2": f"inputs larger than L2: the {prm.num_rows * prm.num_cols * prm.n1 * 8 / (1 << 30):g} GiB prepared DB "
+                  "is streamed every step"}
 
 
 # ---------------------------------------------------------------------------
@@ -270,6 +275,45 @@ def gpu_arm(args, prm):
         e2e_el = float(t.item())
     e2e_value = n_answers / e2e_el
 
+    # ---- batched: B independent queries per step share one database pass.
+    batched = None
+    if args.batch > 1:
+        B = args.batch
+        check(L.via_server_reserve(server._h, B))
+        qb = np.tile(query, B)
+        d_qb = torch.from_numpy(qb.view(np.int64)).cuda()
+        d_mb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
+        d_bb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
+
+        def answer_many():
+            check(L.via_server_answer_many_dev(server._h, ctypes.c_void_p(d_qb.data_ptr()), B, prm.n_lwe,
+                                               ctypes.c_void_p(d_mb.data_ptr()), ctypes.c_void_p(d_bb.data_ptr()),
+                                               sptr))
+
+        for _ in range(2):
+            answer_many()
+        kb = max(2, args.steps // 4)
+        bev = [torch.cuda.Event(enable_timing=True) for _ in range(kb + 1)]
+        if dist:
+            dist.barrier()
+        torch.cuda.synchronize()
+        bev[0].record(stream)
+        for k in range(kb):
+            answer_many()
+            bev[k + 1].record(stream)
+        torch.cuda.synchronize()
+        b_ms = [bev[k].elapsed_time(bev[k + 1]) for k in range(kb)]
+        b_el = bev[0].elapsed_time(bev[-1]) / 1e3
+        if dist:
+            t = torch.tensor([b_el], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            b_el = float(t.item())
+        b_value = kb * B * world / b_el
+        batched = {"answers_s": b_value, "batch": B, "steps": kb, "ms_per_batch": b_el / kb * 1e3,
+                   "db_gbs": b_value * db_bytes / 1e9 / B, "p50_ms": float(np.percentile(b_ms, 50)),
+                   "p99_ms": float(np.percentile(b_ms, 99)), "vs_plain": b_value / value}
+        del d_qb, d_mb, d_bb
+
     # ---- roofline of the dominant kernel: the FirstDim scan alone, timed live.
     sel = torch.randint(0, prm.q2, (prm.num_rows * 2 * prm.n1,), dtype=torch.int64, device="cuda")
     out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
@@ -298,10 +342,10 @@ def gpu_arm(args, prm):
             "config": config_dict(prm),
             "plain": {"answers_s": value, "db_gbs": value * db_bytes / 1e9, "db_raw_gbs": value * (1 << 30) / 1e9,
                       "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
-            "batched": None,
+            "batched": batched,
             "roofline": {"bound": "hbm", "kernel": "k_first_dim_ntt (FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": SCAN_TRAFFIC_BYTES, "launch_ms": scan_s * 1e3,
+                         "traffic": SCAN_TRAFFIC_BYTES_SMALL * prm.num_rows * prm.num_cols / SCAN_TRAFFIC_CELLS_SMALL, "launch_ms": scan_s * 1e3,
                          "algorithmic_bytes": scan_bytes},
             "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
                     "d2h_bytes_per_step": int(2 * prm.n2 * 8)},

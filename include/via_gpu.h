@@ -135,6 +135,25 @@ via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lw
 via_status via_server_answer_dev(via_server* s, const uint64_t* query, uint64_t n_lwe, uint64_t* out_mask,
                                  uint64_t* out_body, void* stream);
 
+/*
+ * Many independent VIA-C queries answered together: one pass over the
+ * database serves the whole batch (FirstDim is linear, so each column sum is
+ * the same as answering alone), and every other step runs on all queries'
+ * ciphertexts at once. `queries` holds n_queries queries back to back;
+ * out_masks / out_bodies receive n_queries answers of n2 residues each. The
+ * results equal n_queries calls of via_server_answer. Host buffers.
+ */
+via_status via_server_answer_many(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                  uint64_t* out_masks, uint64_t* out_bodies);
+
+/* The same on device buffers, enqueued on `stream`. */
+via_status via_server_answer_many_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                      uint64_t* out_masks, uint64_t* out_bodies, void* stream);
+
+/* Sizes the per-handle workspace for batches of up to max_queries (it also
+ * grows on demand). */
+via_status via_server_reserve(via_server* s, uint64_t max_queries);
+
 void via_server_destroy(via_server* s);
 
 /* Message for the last failing call on this thread ("" if none). */

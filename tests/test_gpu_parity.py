@@ -114,3 +114,20 @@ def test_answer_rejects_wrong_query_length(oracle):
     q = client.query(0, b"qlm-q")
     with pytest.raises(QueryLengthMismatch):
         gpu.answer(q[: -prm.lwe_len])
+
+
+@pytest.mark.parametrize("preset", ["n8", "toy", "paper"])
+def test_answer_many_equals_single_answers(oracle, preset):
+    """A batch shares one database pass; every answer equals the oracle's single answer."""
+    prm = {"n8": n8_preset(), "toy": toy_preset(4, 8), "paper": paper_preset(8, 16)}[preset]
+    rng = np.random.default_rng(99)
+    records = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client, gpu, cpu = _setup(oracle, prm, records, b"many-%s" % preset.encode())
+    for nq in (1, 3, 9):  # exercises the 8-, 4- and 1-query scan kernels
+        idx = [int(i) for i in rng.integers(prm.capacity, size=nq)]
+        qs = np.stack([client.query(i, b"mq-%d-%d" % (nq, k)) for k, i in enumerate(idx)])
+        gm, gb = gpu.answer_many(qs)
+        for k, i in enumerate(idx):
+            cm, cb = cpu.answer(qs[k])
+            assert np.array_equal(gm[k], cm) and np.array_equal(gb[k], cb), (nq, k)
+            assert np.array_equal(client.recover(gm[k], gb[k]), records[i])

@@ -57,6 +57,13 @@ def lib() -> ctypes.CDLL:
     L.via_first_dim_scan_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_debug_stage.restype = ctypes.c_int
     L.via_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_uint64]
+    L.via_server_answer_many.restype = ctypes.c_int
+    L.via_server_answer_many.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_uint64, _u64p, _u64p]
+    L.via_server_answer_many_dev.restype = ctypes.c_int
+    L.via_server_answer_many_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                             ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_server_reserve.restype = ctypes.c_int
+    L.via_server_reserve.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
     L.via_kernel_launches.restype = ctypes.c_uint64
     L.via_kernel_launches.argtypes = []
     _lib = L

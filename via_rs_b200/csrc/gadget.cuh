@@ -6,6 +6,7 @@
 #pragma once
 #include <cmath>
 
+#include "ntt.cuh"
 #include "server.cuh"
 
 namespace via {
@@ -134,14 +135,15 @@ __host__ __device__ __forceinline__ u64 digits64(u64 u, int cnt, const Gadget& g
   return u;
 }
 
-// Digits of one coefficient given its residues (nl limbs). Writes L signed
-// digits, d[k] = k-th least significant (pairs with sample L-1-k).
-__host__ __device__ void decompose_coeff(u64 a0, u64 a1, const DevRing& R, const Gadget& g, i64* d) {
-  // Centred lift: v <= Q/2 ? v : v - Q.
+// The scaled value of one coefficient reduced mod B^L into [0, B^L): the
+// centred lift c (v <= Q/2 ? v : v - Q), then round(|c| B^L / Q) with c's sign
+// (gadget.rs:115-151). The balanced digits (gadget.rs:168-190) depend only on
+// this value mod B^L.
+__host__ __device__ __forceinline__ u128 gadget_scaled(u64 a0, u64 a1, const DevRing& R, const Gadget& g) {
   u128 v = R.nl == 2 ? crt2(a0, a1, R) : (u128)a0;
   bool neg = v > g.halfQ;
   u128 mag = neg ? g.Q - v : v;
-  // scaled = floor((mag * S + floor(Q/2)) / Q), exact (wide.rs:145-153).
+  // floor((mag * S + floor(Q/2)) / Q), exact (wide.rs:145-153).
   u128 qe = double_to_u128(u128_to_double(mag) * g.dS_over_Q);
   i128 r = (i128)(mag * g.S + g.halfQ - qe * g.Q);
   i128 qc = (i128)(i64)floor(i128_to_double(r) / g.dQ);
@@ -155,17 +157,42 @@ __host__ __device__ void decompose_coeff(u64 a0, u64 a1, const DevRing& R, const
     r -= (i128)g.Q;
     qe += 1;
   }
-  // Balanced digits depend only on the value mod B^L; take it non-negative.
-  u128 u = (neg && qe != 0) ? g.S - qe : qe;
+  return (neg && qe != 0) ? g.S - qe : qe;
+}
+
+// Splits the scaled value into the two 64-bit chunks the digit loop consumes:
+// lo < B^c holds digits 0..c-1, hi holds digits c..L-1 (plus lo's carry).
+__host__ __device__ __forceinline__ void gadget_chunks(u128 u, const Gadget& g, u64& lo, u64& hi) {
   if (g.c >= g.L) {
-    digits64((u64)u, g.L, g, d);
+    lo = (u64)u;
+    hi = 0;
   } else {
     u128 uh = div_exact(u, (u128)g.Bc, g.dBc);
-    u64 ul = (u64)(u - uh * (u128)g.Bc);
-    u64 carry = digits64(ul, g.c, g, d);
-    digits64((u64)uh + carry, g.L - g.c, g, d + g.c);
+    lo = (u64)(u - uh * (u128)g.Bc);
+    hi = (u64)uh;
   }
 }
 
+// Next balanced digit (k-th, LSB first) from the running chunk value `cur`;
+// at k == c the high chunk takes over with the low chunk's carry.
+__host__ __device__ __forceinline__ i64 gadget_next_digit(u64& cur, u64 hi, int k, const Gadget& g) {
+  if (k == g.c) cur = hi + cur;
+  u64 r;
+  u64 q = divB(cur, g, r);
+  if (r > g.half_base) {
+    cur = q + 1;
+    return (i64)r - (i64)g.base;
+  }
+  cur = q;
+  return (i64)r;
+}
+
+// Digits of one coefficient given its residues (nl limbs). Writes L signed
+// digits, d[k] = k-th least significant (pairs with sample L-1-k).
+__host__ __device__ inline void decompose_coeff(u64 a0, u64 a1, const DevRing& R, const Gadget& g, i64* d) {
+  u64 cur, hi;
+  gadget_chunks(gadget_scaled(a0, a1, R, g), g, cur, hi);
+  for (int k = 0; k < g.L; ++k) d[k] = gadget_next_digit(cur, hi, k, g);
+}
 
 }  // namespace via

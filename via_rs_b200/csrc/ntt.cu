@@ -114,58 +114,6 @@ constexpr int NTT_THREADS = 256;
 // sub-blocks u; a thread owns 8 >> r consecutive sub-blocks.
 // ---------------------------------------------------------------------------
 template <int LOGN, bool INV, int P>
-struct NttPhase {
-  static constexpr int n = 1 << LOGN;
-  static constexpr int S0 = 3 * P;
-  static constexpr int R = (LOGN - S0) < 3 ? (LOGN - S0) : 3;
-  static constexpr int NSUB = 8 >> R;
-  // Smallest stage len of the phase (see k_ntt_reg).
-  static constexpr int STRIDE = INV ? (1 << S0) : ((n >> (S0 + 1)) >> (R - 1));
-
-  __device__ __forceinline__ static int index(int v, int tid) {
-    const int sub = v >> R, k = v & ((1 << R) - 1);
-    const int u = tid * NSUB + sub;
-    return (u / STRIDE) * (STRIDE << R) + (u % STRIDE) + k * STRIDE;
-  }
-
-  __device__ __forceinline__ static void run(u64 (&e)[8], int tid, const NttTable& T) {
-    const u64 q = T.q;
-#pragma unroll
-    for (int sub = 0; sub < NSUB; ++sub) {
-      const int u = tid * NSUB + sub;
-      const int base = (u / STRIDE) * (STRIDE << R) + (u % STRIDE);
-#pragma unroll
-      for (int lvl = 0; lvl < R; ++lvl) {
-        // forward: len = STRIDE << (R-1-lvl) (decreasing); inverse: STRIDE << lvl.
-        const int hk = INV ? (1 << lvl) : (1 << (R - 1 - lvl));
-        const int len = STRIDE * hk;
-        const int m = n / (2 * len);
-#pragma unroll
-        for (int k = 0; k < (1 << R); ++k) {
-          if (k & hk) continue;
-          const int x = base + k * STRIDE;
-          const int grp = x / (2 * len);
-          u64& a = e[sub * (1 << R) + k];
-          u64& c = e[sub * (1 << R) + k + hk];
-          if (!INV) {
-            const u64 w = __ldg(T.psi + m + grp), ws = __ldg(T.psi_sh + m + grp);
-            const u64 t = mul_shoup(c, w, ws, q);
-            const u64 av = a;
-            a = addmod(av, t, q);
-            c = submod(av, t, q);
-          } else {
-            const u64 w = __ldg(T.ipsi + m + grp), ws = __ldg(T.ipsi_sh + m + grp);
-            const u64 av = a, cv = c;
-            a = addmod(av, cv, q);
-            c = mul_shoup(submod(av, cv, q), w, ws, q);
-          }
-        }
-      }
-    }
-  }
-};
-
-template <int LOGN, bool INV, int P>
 __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* ssm, bool active) {
   using Ph = NttPhase<LOGN, INV, P>;
   constexpr int NPH = (LOGN + 2) / 3;

@@ -33,6 +33,88 @@ struct NttTableHost {
   bool valid = false;
 };
 
+// One phase (up to three butterfly stages) of the register-resident transform:
+// each thread holds 8 residues of a length-2^LOGN segment. Stage s of the
+// forward transform pairs (x, x + len_s), len_s = n >> (s+1), with twiddle
+// psi[n/(2 len_s) + x/(2 len_s)] (Cooley-Tukey, bit-reversed twiddles); the
+// inverse runs len = 1, 2, ..., n/2 (Gentleman-Sande, psi^-1). Phase P covers
+// stages 3P..3P+R-1 and works on sub-blocks of 2^R residues x = base + k*STRIDE,
+// where STRIDE is the phase's smallest len and base = (u / STRIDE) *
+// (STRIDE << R) + u % STRIDE over the n >> R sub-blocks u; a thread owns
+// 8 >> R consecutive sub-blocks.
+template <int LOGN, bool INV, int P>
+struct NttPhase {
+  static constexpr int n = 1 << LOGN;
+  static constexpr int S0 = 3 * P;
+  static constexpr int R = (LOGN - S0) < 3 ? (LOGN - S0) : 3;
+  static constexpr int NSUB = 8 >> R;
+  // Smallest stage len of the phase (see k_ntt_reg).
+  static constexpr int STRIDE = INV ? (1 << S0) : ((n >> (S0 + 1)) >> (R - 1));
+
+  __device__ __forceinline__ static int index(int v, int tid) {
+    const int sub = v >> R, k = v & ((1 << R) - 1);
+    const int u = tid * NSUB + sub;
+    return (u / STRIDE) * (STRIDE << R) + (u % STRIDE) + k * STRIDE;
+  }
+
+  __device__ __forceinline__ static void run(u64 (&e)[8], int tid, const NttTable& T) {
+    const u64 q = T.q;
+#pragma unroll
+    for (int sub = 0; sub < NSUB; ++sub) {
+      const int u = tid * NSUB + sub;
+      const int base = (u / STRIDE) * (STRIDE << R) + (u % STRIDE);
+#pragma unroll
+      for (int lvl = 0; lvl < R; ++lvl) {
+        // forward: len = STRIDE << (R-1-lvl) (decreasing); inverse: STRIDE << lvl.
+        const int hk = INV ? (1 << lvl) : (1 << (R - 1 - lvl));
+        const int len = STRIDE * hk;
+        const int m = n / (2 * len);
+#pragma unroll
+        for (int k = 0; k < (1 << R); ++k) {
+          if (k & hk) continue;
+          const int x = base + k * STRIDE;
+          const int grp = x / (2 * len);
+          u64& a = e[sub * (1 << R) + k];
+          u64& c = e[sub * (1 << R) + k + hk];
+          if (!INV) {
+            const u64 w = __ldg(T.psi + m + grp), ws = __ldg(T.psi_sh + m + grp);
+            const u64 t = mul_shoup(c, w, ws, q);
+            const u64 av = a;
+            a = addmod(av, t, q);
+            c = submod(av, t, q);
+          } else {
+            const u64 w = __ldg(T.ipsi + m + grp), ws = __ldg(T.ipsi_sh + m + grp);
+            const u64 av = a, cv = c;
+            a = addmod(av, cv, q);
+            c = mul_shoup(submod(av, cv, q), w, ws, q);
+          }
+        }
+      }
+    }
+  }
+};
+
+
+// Forward transform of a segment whose residues a thread already holds in the
+// phase-0 layout (NttPhase<LOGN,false,0>::index); leaves them in the layout of
+// the last phase. `ssm` is the segment's n-residue shared-memory exchange area.
+template <int LOGN, int P = 0>
+__device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const NttTable& T, u64* ssm) {
+  using Ph = NttPhase<LOGN, false, P>;
+  constexpr int NPH = (LOGN + 2) / 3;
+  Ph::run(e, tid, T);
+  if constexpr (P + 1 < NPH) {
+    using Nx = NttPhase<LOGN, false, P + 1>;
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = ssm[Nx::index(v, tid)];
+    ntt_forward_regs<LOGN, P + 1>(e, tid, T, ssm);
+  }
+}
+
 // Builds tables for q (prime, 2*nmax | q-1). Returns valid=false otherwise.
 NttTableHost make_ntt_table(u64 q, int nmax);
 void free_ntt_table(NttTableHost& t);

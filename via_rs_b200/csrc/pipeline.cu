@@ -34,36 +34,47 @@ __global__ void k_decompose(const u64* __restrict__ in, int n_in, int stride, lo
   const int nl = R.nl;
   const u64* src = in + p * nl * n_in;
   u64 a0 = src[i], a1 = nl == 2 ? src[n_in + i] : 0;
-  i64 d[64];
-  decompose_coeff(a0, a1, R, g, d);
+  u64 cur, hi;
+  gadget_chunks(gadget_scaled(a0, a1, R, g), g, cur, hi);
   const int n_out = n_in * stride;
-  u64* dst = out + p * (long)g.L * nl * n_out;
+  u64* dst = out + p * (long)g.L * nl * n_out + (long)i * stride;
   for (int k = 0; k < g.L; ++k) {
-    int s = g.L - 1 - k;
+    const i64 d = gadget_next_digit(cur, hi, k, g);
+    const int s = g.L - 1 - k;
     for (int l = 0; l < nl; ++l) {
-      u64* o = dst + ((long)s * nl + l) * n_out + (long)i * stride;
-      o[0] = lift_i64(d[k], R.m[l]);
+      u64* o = dst + ((long)s * nl + l) * n_out;
+      o[0] = lift_i64(d, R.m[l]);
       for (int z = 1; z < stride; ++z) o[z] = 0;
     }
   }
 }
 
+// Which eval-form key samples output o multiplies: K_o = base + ((o / div) % mod) * stride.
+// stride = 0 means "consecutive keys" (T*2*nl*n residues apart, T = samples per key).
+struct KeySel {
+  const u64* base;
+  long div, mod, stride;
+};
+static inline KeySel keys_shared(const u64* base) { return KeySel{base, 1, 1, 0}; }
+static inline KeySel keys_cyclic(const u64* base, long mod) { return KeySel{base, 1, mod, 0}; }
+
 // ---------------------------------------------------------------------------
 // Multiply-accumulate against eval-form keys.
 //   out[o].{mask,body} = sum_{s<T} D[o*T + s] (*) K_o[s].{mask,body}
-// K_o = K + key_id(o) * T*2*nl*n with key_id(o) = (o / kdiv) % kmod.
+// K_o selected by a KeySel (T samples per key).
 // ---------------------------------------------------------------------------
-__global__ void k_mac_ntt(const u64* __restrict__ D, const u64* __restrict__ K, u64* __restrict__ out, int T, int n,
-                          int nl, long nout, long kdiv, long kmod, DevRing R) {
+__global__ void k_mac_ntt(const u64* __restrict__ D, KeySel ks, u64* __restrict__ out, int T, int n, int nl, long nout,
+                          DevRing R) {
   long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long per = (long)nl * n;
   if (gid >= nout * per) return;
   long o = gid / per;
   int rem = (int)(gid % per);
   int l = rem / n;
-  const u64* Ko = K + ((o / kdiv) % kmod) * (long)T * 2 * per;
+  const u64* Ko = ks.base + ((o / ks.div) % ks.mod) * (ks.stride ? ks.stride : (long)T * 2 * per);
   const u64* Do = D + o * (long)T * per;
   Acc128 am{0, 0}, ab{0, 0};
+#pragma unroll 6
   for (int s = 0; s < T; ++s) {
     u64 dv = Do[s * per + rem];
     mac128(am, dv, Ko[(2 * s) * per + rem]);
@@ -75,15 +86,15 @@ __global__ void k_mac_ntt(const u64* __restrict__ D, const u64* __restrict__ K, 
 }
 
 // Schoolbook (non-NTT ring) variant: negacyclic products, exact.
-__global__ void k_mac_schoolbook(const u64* __restrict__ D, const u64* __restrict__ K, u64* __restrict__ out, int T,
-                                 int n, int nl, long nout, long kdiv, long kmod, DevRing R) {
+__global__ void k_mac_schoolbook(const u64* __restrict__ D, KeySel ks, u64* __restrict__ out, int T, int n, int nl,
+                                 long nout, DevRing R) {
   long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   long per = (long)nl * n;
   if (gid >= nout * per) return;
   long o = gid / per;
   int rem = (int)(gid % per);
   int l = rem / n, t = rem % n;
-  const u64* Ko = K + ((o / kdiv) % kmod) * (long)T * 2 * per;
+  const u64* Ko = ks.base + ((o / ks.div) % ks.mod) * (ks.stride ? ks.stride : (long)T * 2 * per);
   const u64* Do = D + o * (long)T * per;
   const DevMod& m = R.m[l];
   const bool pow2 = m.log2q >= 0;
@@ -139,6 +150,15 @@ __global__ void k_rlwe_addsub(u64* out, const u64* a, long sa, const u64* b, lon
   u64 q = R.m[l].q;
   u64 x = a[j * sa * per + rem], y = b[j * sb * per + rem];
   out[j * per + rem] = sign > 0 ? addmod(x, y, q) : submod(x, y, q);
+}
+
+// The trivial RLWE (0, delta) at q1 (answer.rs:181-191): zero mask, body = delta * X^0.
+__global__ void k_set_trivial(u64* ct, int n, int nl, u64 d0, u64 d1) {
+  int gid = blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= 2 * nl * n) return;
+  int poly = gid / (nl * n), rem = gid % (nl * n);
+  int l = rem / n, i = rem % n;
+  ct[gid] = (poly == 1 && i == 0) ? (l == 0 ? d0 : d1) : 0;
 }
 
 // DMux combine (mux.rs:129-137, 222-251): out[2j] = in[j] - ext[j], out[2j+1] = ext[j].
@@ -335,13 +355,13 @@ __global__ void k_ring_switch_finish(const u64* acc, const u64* body_proj, int n
 static inline unsigned blocks(long items, int threads = 256) { return (unsigned)((items + threads - 1) / threads); }
 
 struct Workspace {
-  // Sizes.
-  long nlwe = 0, nbits = 0;
+  long nlwe = 0, nbits = 0;  // per query
+  int bmax = 1;              // queries the buffers are sized for
   // Cascade.
   DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
   // RLWE -> RGSW.
-  DevBuf g_digits, g_gp, rgsw_q1;  // rgsw_q1: [nbits][2L][2][nl][n1]
-  DevBuf rgsw_q2;                  // cmux + crot bits at q2
+  DevBuf g_digits, g_gp, rgsw_q1;  // rgsw_q1: [q][nbits][2L][2][nl][n1]
+  DevBuf rgsw_q2;                  // all bits mod-switched to q2: [q][nbits][2L][2][n1]
   // DMux.
   DevBuf dm_a, dm_b, dm_digits, dm_ext;
   // FirstDim / CMux.
@@ -349,6 +369,13 @@ struct Workspace {
   // CRot / RespComp.
   DevBuf cr_ct, cr_diff, cr_digits, cr_ext, rs_ct3, rs_mproj, rs_bproj, rs_digits, rs_gp, rs_acc;
   Gadget g_ck, g_dmux, g_cmux, g_rsk;
+  // Staging for the captured answer graphs: queries in, answers out.
+  DevBuf q_in, a_mask, a_body;
+  std::vector<std::pair<int, cudaGraphExec_t>> graphs;  // one per batch size
+  std::vector<std::pair<int, unsigned long long>> graph_kernels;
+  ~Workspace() {
+    for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+  }
 };
 
 void WorkspaceDeleter::operator()(Workspace* w) const { delete w; }
@@ -385,13 +412,15 @@ void autotune_first_dim(Server& s) {
   cudaEventDestroy(e1);
 }
 
-void workspace_create(Server& s) {
+void workspace_create(Server& s, int bmax) {
   const via_params& p = s.prm;
   auto w = std::make_unique<Workspace>();
   const long n1 = p.n1, n2 = p.n2, nl = s.r1.nl, L = p.l_query, Lck = p.l_ck, I = p.num_rows, J = p.num_cols;
+  const long B = std::max(1, bmax);
+  w->bmax = (int)B;
   w->nlwe = (long)query_lwes(p);
   w->nbits = w->nlwe / L;
-  const long nlwe = w->nlwe;
+  const long nlwe = w->nlwe * B;  // LWEs of a full batch
   w->c_masks_a.alloc(nlwe * n1 * nl);
   w->c_masks_b.alloc(nlwe * n1 * nl);
   w->c_body_a.alloc(nlwe * n1 * nl);
@@ -402,36 +431,41 @@ void workspace_create(Server& s) {
   w->c_rlwe.alloc(nlwe * 2 * n1 * nl);
   w->g_digits.alloc(nlwe * Lck * nl * n1);
   w->g_gp.alloc(nlwe * 2 * nl * n1);
-  w->rgsw_q1.alloc(w->nbits * 2 * L * 2 * nl * n1);
-  w->rgsw_q2.alloc(w->nbits * 2 * L * 2 * n1);
-  w->dm_a.alloc(I * 2 * nl * n1);
-  w->dm_b.alloc(I * 2 * nl * n1);
-  w->dm_digits.alloc(std::max(1L, I / 2) * 2 * L * nl * n1);
-  w->dm_ext.alloc(std::max(1L, I / 2) * 2 * nl * n1);
-  w->sel.alloc(I * 2 * n1);
-  w->sel_split.alloc(I * 2 * n1);  // uint2 per residue
-  w->fd_out.alloc(J * 2 * n1);
-  w->cm_diff.alloc(std::max(1L, J / 2) * 2 * n1);
-  w->cm_digits.alloc(std::max(1L, J / 2) * 2 * L * n1);
-  w->cm_ext.alloc(std::max(1L, J / 2) * 2 * n1);
-  w->cm_b.alloc(std::max(1L, J / 2) * 2 * n1);
-  w->cr_ct.alloc(2 * n1);
-  w->cr_diff.alloc(2 * n1);
-  w->cr_digits.alloc(2 * L * n1);
-  w->cr_ext.alloc(2 * n1);
-  w->rs_ct3.alloc(2 * n1);
+  w->rgsw_q1.alloc(B * w->nbits * 2 * L * 2 * nl * n1);
+  w->rgsw_q2.alloc(B * w->nbits * 2 * L * 2 * n1);
+  w->dm_a.alloc(B * I * 2 * nl * n1);
+  w->dm_b.alloc(B * I * 2 * nl * n1);
+  w->dm_digits.alloc(B * std::max(1L, I / 2) * 2 * L * nl * n1);
+  w->dm_ext.alloc(B * std::max(1L, I / 2) * 2 * nl * n1);
+  w->sel.alloc(B * I * 2 * n1);
+  w->sel_split.alloc(B * I * 2 * n1);  // uint2 per residue
+  w->fd_out.alloc(B * J * 2 * n1);
+  w->cm_diff.alloc(B * std::max(1L, J / 2) * 2 * n1);
+  w->cm_digits.alloc(B * std::max(1L, J / 2) * 2 * L * n1);
+  w->cm_ext.alloc(B * std::max(1L, J / 2) * 2 * n1);
+  w->cm_b.alloc(B * std::max(1L, J / 2) * 2 * n1);
+  w->cr_ct.alloc(B * 2 * n1);
+  w->cr_diff.alloc(B * 2 * n1);
+  w->cr_digits.alloc(B * 2 * L * n1);
+  w->cr_ext.alloc(B * 2 * n1);
+  w->rs_ct3.alloc(B * 2 * n1);
   long d = n1 / n2;
-  w->rs_mproj.alloc(d * n2);
-  w->rs_bproj.alloc(n2);
-  w->rs_digits.alloc(d * p.l_rsk * n2);
-  w->rs_gp.alloc(d * 2 * n2);
-  w->rs_acc.alloc(2 * n2);
+  w->rs_mproj.alloc(B * d * n2);
+  w->rs_bproj.alloc(B * n2);
+  w->rs_digits.alloc(B * d * p.l_rsk * n2);
+  w->rs_gp.alloc(B * d * 2 * n2);
+  w->rs_acc.alloc(B * 2 * n2);
+  w->q_in.alloc(nlwe * lwe_len(p));
+  w->a_mask.alloc(B * n2);
+  w->a_body.alloc(B * n2);
   w->g_ck = make_gadget(p.ck_base, (int)p.l_ck, s.r1.Q());
   w->g_dmux = make_gadget(p.b_dmux, (int)p.l_query, s.r1.Q());
   w->g_cmux = make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q());
   w->g_rsk = make_gadget(p.b_rsk, (int)p.l_rsk, s.r3.Q());
   s.ws.reset(w.release());
 }
+
+int workspace_batch(Server& s) { return s.ws ? s.ws->bmax : 0; }
 
 static void to_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
   if (R.ntt) ntt_forward(data, n, R.nl, segments, R.t[0], R.t[1], st);
@@ -442,13 +476,12 @@ static void from_eval(const DevRing& R, u64* data, int n, long segments, cudaStr
 
 // Gadget products of `nout` outputs with T digit polys each (already in the eval
 // domain) against keys: out eval [nout][2][nl][n].
-static void mac(const DevRing& R, const u64* D, const u64* K, u64* out, int T, int n, long nout, long kdiv, long kmod,
-                cudaStream_t st) {
+static void mac(const DevRing& R, const u64* D, KeySel ks, u64* out, int T, int n, long nout, cudaStream_t st) {
   long items = nout * R.nl * n;
   if (R.ntt)
-    k_mac_ntt<<<blocks(items), 256, 0, st>>>(D, K, out, T, n, R.nl, nout, kdiv, kmod, R);
+    k_mac_ntt<<<blocks(items), 256, 0, st>>>(D, ks, out, T, n, R.nl, nout, R);
   else
-    k_mac_schoolbook<<<blocks(items), 256, 0, st>>>(D, K, out, T, n, R.nl, nout, kdiv, kmod, R);
+    k_mac_schoolbook<<<blocks(items), 256, 0, st>>>(D, ks, out, T, n, R.nl, nout, R);
   VIA_LAUNCHED();
 }
 
@@ -456,6 +489,16 @@ static void decompose(const DevRing& R, const Gadget& g, const u64* in, int n_in
                       cudaStream_t st) {
   k_decompose<<<blocks(npolys * n_in, 128), 128, 0, st>>>(in, n_in, stride, npolys, R, g, out);
   VIA_LAUNCHED();
+}
+
+// Gadget products of `nout` outputs, each summing G decomposed input polys
+// against its eval-form key samples: decompose -> transform -> multiply-accumulate
+// through the `digits` scratch ([nout][G][L][nl][n]).
+static void gadget_product(const DevRing& R, const Gadget& g, const u64* in, int n, int stride, int G, long nout,
+                           KeySel ks, u64* out, u64* digits, cudaStream_t st) {
+  decompose(R, g, in, n / stride, stride, (long)G * nout, digits, st);
+  to_eval(R, digits, n, (long)G * nout * g.L * R.nl, st);
+  mac(R, digits, ks, out, G * g.L, n, nout, st);
 }
 
 static double to_double(u128 x) { return (double)(u64)(x >> 64) * 18446744073709551616.0 + (double)(u64)x; }
@@ -466,13 +509,13 @@ static void mod_switch(const DevRing& S, const u64* in, const DevRing& D, u64* o
   VIA_LAUNCHED();
 }
 
-// Step 1: QueryDecomp -> rgsw_q1 [nbits][2L][2][nl][n1] (coefficient form).
-static void query_decomp(Server& s, const u64* d_query, cudaStream_t st) {
+// Step 1: QueryDecomp for nq queries -> rgsw_q1 [q][nbits][2L][2][nl][n1] (coefficient form).
+static void query_decomp(Server& s, const u64* d_query, int nq, cudaStream_t st) {
   Workspace& w = *s.ws;
   const via_params& p = s.prm;
   const DevRing& R = s.r1;
   const int n1 = p.n1, nl = R.nl, L = p.l_ck;
-  const long nlwe = w.nlwe;
+  const long nlwe = w.nlwe * nq;
   k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query, n1, nl, nlwe, w.c_masks_a.p, w.c_body_a.p);
   VIA_LAUNCHED();
   u64 *mi = w.c_masks_a.p, *mo = w.c_masks_b.p, *bi = w.c_body_a.p, *bo = w.c_body_b.p;
@@ -481,9 +524,8 @@ static void query_decomp(Server& s, const u64* d_query, cudaStream_t st) {
   for (int n_in = 1; n_in < n1; n_in <<= 1, ++k) {
     const int n_out = 2 * n_in, rank_in = n1 / n_in;
     const long polys = nlwe * rank_in;
-    decompose(R, w.g_ck, mi, n_in, 2, polys, w.c_digits.p, st);
-    to_eval(R, w.c_digits.p, n_out, polys * L * nl, st);
-    mac(R, w.c_digits.p, s.cascade_eval.p + k * step_len, w.c_P.p, L, n_out, polys, 1, rank_in, st);
+    gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), w.c_P.p,
+                   w.c_digits.p, st);
     const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
     k_cascade_reduce<<<blocks(items), 256, 0, st>>>(w.c_P.p, rank_in, n_out, nl, nlwe, R, mo, w.c_bsum.p);
     VIA_LAUNCHED();
@@ -496,146 +538,239 @@ static void query_decomp(Server& s, const u64* d_query, cudaStream_t st) {
   }
   k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, w.c_rlwe.p);
   VIA_LAUNCHED();
-  // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178):
-  // decompose every RLWE mask (its polys are at index 2w of c_rlwe).
-  const int Lq = p.l_query;
-  // The final rank-1 masks are already contiguous [lwe][nl][n1] in `mi`.
-  decompose(R, w.g_ck, mi, n1, 1, nlwe, w.g_digits.p, st);
-  to_eval(R, w.g_digits.p, n1, nlwe * L * nl, st);
-  mac(R, w.g_digits.p, s.conv_eval.p, w.g_gp.p, L, n1, nlwe, 1, 1, st);
+  // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178); the
+  // final rank-1 masks are already contiguous [lwe][nl][n1] in `mi`.
+  gadget_product(R, w.g_ck, mi, n1, 1, 1, nlwe, keys_shared(s.conv_eval.p), w.g_gp.p, w.g_digits.p, st);
   from_eval(R, w.g_gp.p, n1, nlwe * 2 * nl, st);
-  k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(w.c_rlwe.p, w.g_gp.p, Lq, w.nbits, n1, nl, R,
-                                                               w.rgsw_q1.p);
+  k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(w.c_rlwe.p, w.g_gp.p, (int)p.l_query, w.nbits * nq, n1,
+                                                               nl, R, w.rgsw_q1.p);
   VIA_LAUNCHED();
 }
 
-// One external-product level: ext[j] = bit (x) ct[j] for `count` RLWEs (coefficient
-// form in `cts`), result in the eval domain unless `to_coeff`.
-static void external_products(const DevRing& R, const Gadget& g, const u64* rgsw_eval, const u64* cts, long count,
-                              u64* digits, u64* ext, bool to_coeff, cudaStream_t st) {
-  const int n = R.n, L = g.L;
-  // Decompose mask and body of every RLWE: 2*count polys -> L digits each,
-  // giving per RLWE 2L digit polys ordered (mask digits, body digits), which
-  // pair with (neg_s_m samples, m samples) of the RGSW.
-  decompose(R, g, cts, n, 1, 2 * count, digits, st);
-  to_eval(R, digits, n, 2 * count * L * R.nl, st);
-  mac(R, digits, rgsw_eval, ext, 2 * L, n, count, 1, 1, st);
+// ext[o] = bit_o (x) cts[o] for `count` RLWEs (coefficient form); result in the
+// eval domain unless `to_coeff`. The RGSW of output o is selected by `rgsw`.
+static void external_products(const DevRing& R, const Gadget& g, KeySel rgsw, const u64* cts, long count, u64* digits,
+                              u64* ext, bool to_coeff, cudaStream_t st) {
+  const int n = R.n;
+  // Mask and body of every RLWE are the G = 2 decomposed inputs; their digits
+  // pair with the neg_s_m and m samples of the RGSW respectively.
+  gadget_product(R, g, cts, n, 1, 2, count, rgsw, ext, digits, st);
   if (to_coeff) from_eval(R, ext, n, 2 * count * R.nl, st);
 }
 
-void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st) {
-  answer_device_stages(s, d_query, d_mask, d_body, st, 0, nullptr);
+// CRot diff for nq RLWEs: rot = -(X^k * ct), diff = rot - ct.
+__global__ void k_crot_diff_batch(const u64* ct, int n, int k, long nq, DevMod m, u64* diff) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nq * 2 * n) return;
+  long p = gid / n;
+  int i = (int)(gid % n);
+  int src = i - k;
+  bool wrap = src < 0;
+  if (wrap) src += n;
+  u64 v = ct[p * n + src];
+  u64 xk = wrap ? negmod(v, m.q) : v;
+  diff[p * n + i] = submod(negmod(xk, m.q), ct[p * n + i], m.q);
 }
 
-// Runs the pipeline; when stop_stage > 0, copies that stage's output (in
-// coefficient form) to `dump` and returns early. Stages: 1 cascade RLWEs,
-// 2 query RGSWs at q1, 3 DMux outputs, 4 mod-switched rows at q2, 5 FirstDim
-// columns, 6 CMux output, 7 CRot output.
-void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st, int stop_stage,
-                          u64* dump) {
+__global__ void k_ring_switch_proj_batch(const u64* ct, int n1, int n2, long nq, DevMod m, u64* mask_proj,
+                                         u64* body_proj) {
+  const int d = n1 / n2;
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nq * (d + 1) * n2) return;
+  long q = gid / ((d + 1) * n2);
+  int r = (int)(gid % ((d + 1) * n2));
+  int j = r / n2, t = r % n2;
+  const u64* c = ct + q * 2 * n1;
+  if (j == d) {
+    body_proj[q * n2 + t] = c[n1 + d * t];
+    return;
+  }
+  int src = d * t - j;
+  bool wrap = src < 0;
+  if (wrap) src += n1;
+  u64 v = c[src];
+  mask_proj[(q * d + j) * n2 + t] = wrap ? negmod(v, m.q) : v;
+}
+
+__global__ void k_ring_switch_sum_batch(const u64* gp, int d, int n2, long nq, DevMod m, u64* acc) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nq * 2 * n2) return;
+  long q = gid / (2 * n2);
+  int r = (int)(gid % (2 * n2));
+  int mb = r / n2, t = r % n2;
+  u64 sacc = 0;
+  for (int j = 0; j < d; ++j) sacc = addmod(sacc, gp[((q * d + j) * 2 + mb) * n2 + t], m.q);
+  acc[q * 2 * n2 + mb * n2 + t] = sacc;
+}
+
+__global__ void k_ring_switch_finish_batch(const u64* acc, const u64* body_proj, int n2, long nq, DevMod m3, DevMod m4,
+                                           double dq3, u64* out_mask, u64* out_body) {
+  long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nq * n2) return;
+  long q = gid / n2;
+  int t = (int)(gid % n2);
+  const u64 q3 = m3.q;
+  const u64* a = acc + q * 2 * n2;
+  out_mask[q * n2 + t] = negmod(a[t], q3);  // mask: q3 -> q3 is the identity rescale
+  u64 body = submod(body_proj[q * n2 + t], a[n2 + t], q3);
+  // body: q3 -> q4 (mod_switch_asym, prim/switching/mod_switch.rs:124-154).
+  u128 num = (u128)body * m4.q + q3 / 2;
+  u64 r = (u64)div_exact(num, (u128)q3, dq3);
+  out_body[q * n2 + t] = r >= m4.q ? r - m4.q : r;
+}
+
+// Runs the pipeline for nq queries (d_query: nq queries back to back; d_mask,
+// d_body: [nq][n2]). When stop_stage > 0 (nq == 1 only), copies that stage's
+// output in coefficient form to `dump` and returns early. Stages: 1 cascade
+// RLWEs, 2 query RGSWs at q1, 3 DMux outputs, 4 mod-switched rows at q2,
+// 5 FirstDim columns, 6 CMux output, 7 CRot output.
+void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u64* d_body, cudaStream_t st,
+                          int stop_stage, u64* dump) {
   Workspace& w = *s.ws;
   const via_params& p = s.prm;
   const int n1 = p.n1, n2 = p.n2, L = p.l_query, nl = s.r1.nl;
-  const long I = p.num_rows, J = p.num_cols;
+  const long I = p.num_rows, J = p.num_cols, B = nq;
   const int nd = ilog2(I), nc = ilog2(J);
   const int nr = (int)(w.nbits - nd - nc);
   const long rgsw1 = 2L * L * 2 * nl * n1, rgsw2 = 2L * L * 2 * n1;
-
+  if (nq < 1 || nq > w.bmax) throw CudaError(100, "batch larger than the workspace");
   auto copy_out = [&](const u64* src, size_t count) {
     VIA_CUDA(cudaMemcpyAsync(dump, src, count * 8, cudaMemcpyDeviceToDevice, st));
   };
   // ---- Step 1: QueryDecomp.
-  query_decomp(s, d_query, st);
+  query_decomp(s, d_query, nq, st);
   if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
   if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
 
+  // ---- mod_switch_rgsw q1 -> q2 of every bit (convert.rs:223-240; only the
+  // CMux / CRot bits are used at q2), then eval form for both moduli.
+  mod_switch(s.r1, w.rgsw_q1.p, s.r2, w.rgsw_q2.p, B * w.nbits * 2 * L * 2, n1, st);
+  to_eval(s.r2, w.rgsw_q2.p, n1, B * w.nbits * 2 * L * 2, st);
+  to_eval(s.r1, w.rgsw_q1.p, n1, B * w.nbits * 2 * L * 2 * nl, st);
+
   // ---- Step 2: DMux tree at q1 from the trivial RLWE(0, delta) (answer.rs:181-191).
-  // DMux bits to eval form in place (their coefficient form is no longer needed).
-  to_eval(s.r1, w.rgsw_q1.p, n1, (long)nd * 2 * L * 2 * nl, st);
   {
-    VIA_CUDA(cudaMemsetAsync(w.dm_a.p, 0, 2 * nl * n1 * 8, st));
     u128 Q1 = s.r1.Q();
     u128 delta = (Q1 + p.p - 1) / p.p;
-    for (int l = 0; l < nl; ++l) {
-      u64 v = (u64)(delta % s.r1.m[l].q);
-      VIA_CUDA(cudaMemcpyAsync(w.dm_a.p + (long)(nl + l) * n1, &v, 8, cudaMemcpyHostToDevice, st));
+    for (long q = 0; q < B; ++q) {
+      k_set_trivial<<<blocks(2 * nl * n1), 256, 0, st>>>(w.dm_a.p + q * 2 * nl * n1, n1, nl,
+                                                         (u64)(delta % s.r1.m[0].q), (u64)(delta % s.r1.m[1].q));
+      VIA_LAUNCHED();
     }
     u64 *in = w.dm_a.p, *out = w.dm_b.p;
     for (int i = 0; i < nd; ++i) {
-      long active = 1L << i;
-      external_products(s.r1, w.g_dmux, w.rgsw_q1.p + i * rgsw1, in, active, w.dm_digits.p, w.dm_ext.p, true, st);
-      k_dmux_combine<<<blocks(active * 2 * nl * n1), 256, 0, st>>>(out, in, w.dm_ext.p, active, n1, nl, s.r1);
+      const long active = 1L << i;  // per query
+      KeySel bit{w.rgsw_q1.p + i * rgsw1, active, B, w.nbits * rgsw1};
+      external_products(s.r1, w.g_dmux, bit, in, B * active, w.dm_digits.p, w.dm_ext.p, true, st);
+      k_dmux_combine<<<blocks(B * active * 2 * nl * n1), 256, 0, st>>>(out, in, w.dm_ext.p, B * active, n1, nl, s.r1);
       VIA_LAUNCHED();
       std::swap(in, out);
     }
     if (stop_stage == 3) return copy_out(in, (size_t)I * 2 * nl * n1);
-    // ---- Step 3: ModSwitch q1 -> q2 (answer.rs:194-199) into the selection buffer.
-    mod_switch(s.r1, in, s.r2, w.sel.p, 2 * I, n1, st);
+    // ---- Step 3: ModSwitch q1 -> q2 (answer.rs:194-199) into the selection rows.
+    mod_switch(s.r1, in, s.r2, w.sel.p, B * 2 * I, n1, st);
   }
   if (stop_stage == 4) return copy_out(w.sel.p, (size_t)I * 2 * n1);
 
-  // ---- Step 4: FirstDim (answer.rs:204-205) — result stays in the eval domain.
-  to_eval(s.r2, w.sel.p, n1, 2 * I, st);
-  first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st, workspace_sel_split(s),
-                 s.fd_variant);
+  // ---- Step 4: FirstDim (answer.rs:204-205), one pass over the database for
+  // the whole batch; the columns stay in the eval domain.
+  to_eval(s.r2, w.sel.p, n1, B * 2 * I, st);
+  first_dim_eval_batch(s.db.p, w.sel.p, w.fd_out.p, nq, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st,
+                       workspace_sel_split(s), s.fd_variant);
   if (stop_stage == 5) {
     copy_out(w.fd_out.p, (size_t)J * 2 * n1);
     from_eval(s.r2, dump, n1, 2 * J, st);
     return;
   }
 
-  // ---- CMux / CRot bits: mod_switch_rgsw q1 -> q2 (convert.rs:223-240), then eval.
-  const long nq2 = (long)(nc + nr);
-  if (nq2) {
-    mod_switch(s.r1, w.rgsw_q1.p + nd * rgsw1, s.r2, w.rgsw_q2.p, nq2 * 2 * L * 2, n1, st);
-    to_eval(s.r2, w.rgsw_q2.p, n1, nq2 * 2 * L * 2, st);
-  }
-
   // ---- Step 5: CMux tree (mux.rs:167-198), level by level in the eval domain:
   // diff = in[2j+1] - in[2j] (eval) -> coeff -> gadget product -> out[j] = in[2j] + ext.
   u64* cur = w.fd_out.p;
-  u64* nxt = nullptr;
   for (int i = 0; i < nc; ++i) {
-    long half = (J >> i) / 2;
-    k_rlwe_addsub<<<blocks(half * 2 * n1), 256, 0, st>>>(w.cm_diff.p, cur + 2 * n1, 2, cur, 2, -1, half, n1, 1, s.r2);
+    const long half = (J >> i) / 2;  // CMuxes per query at this level
+    k_rlwe_addsub<<<blocks(B * half * 2 * n1), 256, 0, st>>>(w.cm_diff.p, cur + 2 * n1, 2, cur, 2, -1, B * half, n1, 1,
+                                                             s.r2);
     VIA_LAUNCHED();
-    from_eval(s.r2, w.cm_diff.p, n1, 2 * half, st);
-    external_products(s.r2, w.g_cmux, w.rgsw_q2.p + i * rgsw2, w.cm_diff.p, half, w.cm_digits.p, w.cm_ext.p, false, st);
-    nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
-    k_rlwe_addsub<<<blocks(half * 2 * n1), 256, 0, st>>>(nxt, cur, 2, w.cm_ext.p, 1, +1, half, n1, 1, s.r2);
+    from_eval(s.r2, w.cm_diff.p, n1, B * 2 * half, st);
+    KeySel bit{w.rgsw_q2.p + (nd + i) * rgsw2, half, B, w.nbits * rgsw2};
+    external_products(s.r2, w.g_cmux, bit, w.cm_diff.p, B * half, w.cm_digits.p, w.cm_ext.p, false, st);
+    u64* nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
+    k_rlwe_addsub<<<blocks(B * half * 2 * n1), 256, 0, st>>>(nxt, cur, 2, w.cm_ext.p, 1, +1, B * half, n1, 1, s.r2);
     VIA_LAUNCHED();
     cur = nxt;
   }
-  // Selected column back to coefficient form.
-  VIA_CUDA(cudaMemcpyAsync(w.cr_ct.p, cur, 2 * n1 * 8, cudaMemcpyDeviceToDevice, st));
-  from_eval(s.r2, w.cr_ct.p, n1, 2, st);
+  // Selected columns back to coefficient form.
+  VIA_CUDA(cudaMemcpyAsync(w.cr_ct.p, cur, (size_t)B * 2 * n1 * 8, cudaMemcpyDeviceToDevice, st));
+  from_eval(s.r2, w.cr_ct.p, n1, B * 2, st);
   if (stop_stage == 6) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
 
   // ---- Step 6: CRot, SlotExtract (rotate.rs:128-150).
   for (int i = 0; i < nr; ++i) {
-    k_crot_diff<<<blocks(2 * n1), 256, 0, st>>>(w.cr_ct.p, n1, n1 - (1 << i), s.r2.m[0], w.cr_diff.p);
+    k_crot_diff_batch<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, n1, n1 - (1 << i), B, s.r2.m[0], w.cr_diff.p);
     VIA_LAUNCHED();
-    external_products(s.r2, w.g_cmux, w.rgsw_q2.p + (nc + i) * rgsw2, w.cr_diff.p, 1, w.cr_digits.p, w.cr_ext.p, true,
-                      st);
-    k_rlwe_addsub<<<blocks(2 * n1), 256, 0, st>>>(w.cr_ct.p, w.cr_ct.p, 1, w.cr_ext.p, 1, +1, 1, n1, 1, s.r2);
+    KeySel bit{w.rgsw_q2.p + (nd + nc + i) * rgsw2, 1, B, w.nbits * rgsw2};
+    external_products(s.r2, w.g_cmux, bit, w.cr_diff.p, B, w.cr_digits.p, w.cr_ext.p, true, st);
+    k_rlwe_addsub<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, w.cr_ct.p, 1, w.cr_ext.p, 1, +1, B, n1, 1, s.r2);
     VIA_LAUNCHED();
   }
-
   if (stop_stage == 7) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
+
   // ---- Step 7: RespComp (resp_comp.rs:46-76).
-  mod_switch(s.r2, w.cr_ct.p, s.r3n1, w.rs_ct3.p, 2, n1, st);
+  mod_switch(s.r2, w.cr_ct.p, s.r3n1, w.rs_ct3.p, B * 2, n1, st);
   const int d = n1 / n2;
-  k_ring_switch_proj<<<blocks((d + 1) * n2), 256, 0, st>>>(w.rs_ct3.p, n1, n2, s.r3.m[0], w.rs_mproj.p, w.rs_bproj.p);
+  k_ring_switch_proj_batch<<<blocks(B * (d + 1) * n2), 256, 0, st>>>(w.rs_ct3.p, n1, n2, B, s.r3.m[0], w.rs_mproj.p,
+                                                                      w.rs_bproj.p);
   VIA_LAUNCHED();
-  decompose(s.r3, w.g_rsk, w.rs_mproj.p, n2, 1, d, w.rs_digits.p, st);
-  to_eval(s.r3, w.rs_digits.p, n2, (long)d * p.l_rsk, st);
-  mac(s.r3, w.rs_digits.p, s.rsk_eval.p, w.rs_gp.p, (int)p.l_rsk, n2, d, 1, d, st);
-  k_ring_switch_sum<<<blocks(2 * n2), 256, 0, st>>>(w.rs_gp.p, d, n2, s.r3.m[0], w.rs_acc.p);
+  gadget_product(s.r3, w.g_rsk, w.rs_mproj.p, n2, 1, 1, B * d, keys_cyclic(s.rsk_eval.p, d), w.rs_gp.p,
+                 w.rs_digits.p, st);
+  k_ring_switch_sum_batch<<<blocks(B * 2 * n2), 256, 0, st>>>(w.rs_gp.p, d, n2, B, s.r3.m[0], w.rs_acc.p);
   VIA_LAUNCHED();
-  from_eval(s.r3, w.rs_acc.p, n2, 2, st);
-  k_ring_switch_finish<<<blocks(n2), 256, 0, st>>>(w.rs_acc.p, w.rs_bproj.p, n2, s.r3.m[0], s.r4.m[0],
-                                                   (double)p.q3, d_mask, d_body);
+  from_eval(s.r3, w.rs_acc.p, n2, B * 2, st);
+  k_ring_switch_finish_batch<<<blocks(B * n2), 256, 0, st>>>(w.rs_acc.p, w.rs_bproj.p, n2, B, s.r3.m[0], s.r4.m[0],
+                                                             (double)p.q3, d_mask, d_body);
   VIA_LAUNCHED();
+}
+
+void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st) {
+  answer_device_stages(s, d_query, 1, d_mask, d_body, st, 0, nullptr);
+}
+
+u64* workspace_query(Server& s) { return s.ws->q_in.p; }
+u64* workspace_answer_mask(Server& s) { return s.ws->a_mask.p; }
+u64* workspace_answer_body(Server& s) { return s.ws->a_body.p; }
+
+// The whole answer for nq queries (~220 kernels) on the workspace buffers,
+// captured once per batch size into a CUDA graph and replayed.
+void answer_graph(Server& s, int nq, cudaStream_t st) {
+  Workspace& w = *s.ws;
+  cudaGraphExec_t exec = nullptr;
+  unsigned long long kernels = 0;
+  for (size_t i = 0; i < w.graphs.size(); ++i)
+    if (w.graphs[i].first == nq) {
+      exec = w.graphs[i].second;
+      kernels = w.graph_kernels[i].second;
+    }
+  if (!exec) {
+    cudaGraph_t g;
+    unsigned long long before = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
+    VIA_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+    try {
+      answer_device_stages(s, w.q_in.p, nq, w.a_mask.p, w.a_body.p, s.stream, 0, nullptr);
+    } catch (...) {
+      cudaStreamEndCapture(s.stream, &g);
+      throw;
+    }
+    VIA_CUDA(cudaStreamEndCapture(s.stream, &g));
+    kernels = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED) - before;
+    __atomic_sub_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);  // captured, not run
+    cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
+    cudaGraphDestroy(g);
+    VIA_CUDA(e);
+    w.graphs.push_back({nq, exec});
+    w.graph_kernels.push_back({nq, kernels});
+  }
+  VIA_CUDA(cudaGraphLaunch(exec, st));
+  __atomic_add_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);
 }
 
 }  // namespace via

@@ -234,7 +234,7 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     VIA_CUDA(cudaMemcpyAsync(s.rsk_eval.p, keys->rsk, s.rsk_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
     transform_keys(s);
   }
-  workspace_create(s);
+  workspace_create(s, 1);
   autotune_first_dim(s);
   VIA_CUDA(cudaStreamSynchronize(s.stream));
 }
@@ -291,8 +291,13 @@ via_status via_server_answer_dev(via_server* s, const uint64_t* query, uint64_t 
       throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " + std::to_string(expected) +
                                                         " ciphertexts, got " + std::to_string(n_lwe));
     if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+    const via_params& p = s->prm;
+    cudaStream_t st = (cudaStream_t)stream;
     std::lock_guard<std::mutex> g(s->mu);
-    answer_device(*s, query, out_mask, out_body, (cudaStream_t)stream);
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), query, n_lwe * lwe_len(p) * 8, cudaMemcpyDeviceToDevice, st));
+    answer_graph(*s, 1, st);
+    VIA_CUDA(cudaMemcpyAsync(out_mask, workspace_answer_mask(*s), p.n2 * 8, cudaMemcpyDeviceToDevice, st));
+    VIA_CUDA(cudaMemcpyAsync(out_body, workspace_answer_body(*s), p.n2 * 8, cudaMemcpyDeviceToDevice, st));
   });
 }
 
@@ -320,8 +325,70 @@ via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe,
     std::lock_guard<std::mutex> g(s->mu);
     DevBuf dq(n_lwe * lwe_len(p)), dm(p.n2), db(p.n2), dout(sizes[stage]);
     VIA_CUDA(cudaMemcpyAsync(dq.p, query, dq.n * 8, cudaMemcpyHostToDevice, s->stream));
-    answer_device_stages(*s, dq.p, dm.p, db.p, s->stream, stage, dout.p);
+    answer_device_stages(*s, dq.p, 1, dm.p, db.p, s->stream, stage, dout.p);
     VIA_CUDA(cudaMemcpyAsync(out, dout.p, sizes[stage] * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaStreamSynchronize(s->stream));
+  });
+}
+
+// Grows the workspace (and drops cached graphs) when a batch exceeds it.
+static void ensure_batch(via_server* s, u64 nq) {
+  if ((int)nq <= workspace_batch(*s)) return;
+  VIA_CUDA(cudaStreamSynchronize(s->stream));
+  workspace_destroy(*s);
+  workspace_create(*s, (int)nq);
+}
+
+via_status via_server_reserve(via_server* s, uint64_t max_queries) {
+  return guarded([&] {
+    if (!s || max_queries == 0 || max_queries > 4096) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "bad batch size");
+    std::lock_guard<std::mutex> g(s->mu);
+    ensure_batch(s, max_queries);
+  });
+}
+
+via_status via_server_answer_many_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                      uint64_t* out_masks, uint64_t* out_bodies, void* stream) {
+  return guarded([&] {
+    if (!s || !queries || !out_masks || !out_bodies || n_queries == 0)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+    const via_params& p = s->prm;
+    if (n_lwe != query_lwes(p))
+      throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " +
+                                                        std::to_string(query_lwes(p)) + " ciphertexts, got " +
+                                                        std::to_string(n_lwe));
+    if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(s->mu);
+    ensure_batch(s, n_queries);
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
+                             cudaMemcpyDeviceToDevice, st));
+    answer_graph(*s, (int)n_queries, st);
+    VIA_CUDA(cudaMemcpyAsync(out_masks, workspace_answer_mask(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToDevice, st));
+    VIA_CUDA(cudaMemcpyAsync(out_bodies, workspace_answer_body(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToDevice, st));
+  });
+}
+
+via_status via_server_answer_many(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                  uint64_t* out_masks, uint64_t* out_bodies) {
+  return guarded([&] {
+    if (!s || !queries || !out_masks || !out_bodies || n_queries == 0)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument or empty batch");
+    const via_params& p = s->prm;
+    if (n_lwe != query_lwes(p))
+      throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " +
+                                                        std::to_string(query_lwes(p)) + " ciphertexts, got " +
+                                                        std::to_string(n_lwe));
+    if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+    std::lock_guard<std::mutex> g(s->mu);
+    ensure_batch(s, n_queries);
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
+                             cudaMemcpyHostToDevice, s->stream));
+    answer_graph(*s, (int)n_queries, s->stream);
+    VIA_CUDA(cudaMemcpyAsync(out_masks, workspace_answer_mask(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToHost,
+                             s->stream));
+    VIA_CUDA(cudaMemcpyAsync(out_bodies, workspace_answer_body(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToHost,
+                             s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
   });
 }
@@ -340,11 +407,10 @@ via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lw
     if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
     u64 qlen = n_lwe * lwe_len(p);
     std::lock_guard<std::mutex> g(s->mu);
-    DevBuf dq(qlen), dm(p.n2), db(p.n2);
-    VIA_CUDA(cudaMemcpyAsync(dq.p, query, qlen * 8, cudaMemcpyHostToDevice, s->stream));
-    answer_device(*s, dq.p, dm.p, db.p, s->stream);
-    VIA_CUDA(cudaMemcpyAsync(out_mask, dm.p, p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
-    VIA_CUDA(cudaMemcpyAsync(out_body, db.p, p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), query, qlen * 8, cudaMemcpyHostToDevice, s->stream));
+    answer_graph(*s, 1, s->stream);
+    VIA_CUDA(cudaMemcpyAsync(out_mask, workspace_answer_mask(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaMemcpyAsync(out_body, workspace_answer_body(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
   });
 }

@@ -70,13 +70,18 @@ u64 rsk_len(const via_params& p);
 int ilog2(u64 v);
 
 // Pipeline entry points (pipeline.cu).
-void workspace_create(Server& s);
+void workspace_create(Server& s, int bmax);
+int workspace_batch(Server& s);
 void workspace_destroy(Server& s);
 uint2* workspace_sel_split(Server& s);
+u64* workspace_query(Server& s);
+u64* workspace_answer_mask(Server& s);
+u64* workspace_answer_body(Server& s);
+void answer_graph(Server& s, int nq, cudaStream_t st);
 void autotune_first_dim(Server& s);
 void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st);
-void answer_device_stages(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st, int stop_stage,
-                          u64* dump);
+void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u64* d_body, cudaStream_t st,
+                          int stop_stage, u64* dump);
 
 }  // namespace via
 

@@ -123,6 +123,25 @@ class Server:
         check(_lib.lib().via_server_answer(self._h, _ptr(q), n_lwe, _ptr(mask), _ptr(body)))
         return mask, body
 
+    def answer_many(self, queries):
+        """Answers a batch of independent queries with one shared database pass.
+
+        queries: (n, n_lwe * lwe_len) or flat; returns (masks, bodies), each (n, n2).
+        """
+        prm = self.prm
+        q = _u64(queries).reshape(-1)
+        per = prm.n_lwe * prm.lwe_len
+        if q.size % per:
+            raise BufferTooShort("query buffer is not a whole number of queries")
+        n = q.size // per
+        masks = np.zeros((n, prm.n2), dtype=np.uint64)
+        bodies = np.zeros((n, prm.n2), dtype=np.uint64)
+        check(_lib.lib().via_server_answer_many(self._h, _ptr(q), n, prm.n_lwe, _ptr(masks), _ptr(bodies)))
+        return masks, bodies
+
+    def reserve(self, max_queries: int) -> None:
+        check(_lib.lib().via_server_reserve(self._h, max_queries))
+
     def debug_stage(self, query, stage: int) -> np.ndarray:
         """The answer's intermediate `stage` (1..7), see via_debug_stage in include/via_gpu.h."""
         prm = self.prm
