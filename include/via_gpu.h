@@ -187,6 +187,21 @@ via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint6
 via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe, int stage, uint64_t* out,
                            uint64_t out_len);
 
+/*
+ * The FirstDim scan of via_first_dim_scan_dev for callers that cannot allocate
+ * device memory: code that runs where cudaMalloc is not allowed or not wanted
+ * (inside a region being captured into a CUDA graph, a host whose allocator is
+ * owned by another runtime, a latency-critical path that must not hit the
+ * allocator). It allocates nothing: its scratch (the split selection vectors)
+ * is a static 8 MiB device array that the library holds on every device until
+ * exit, so it requires num_rows * 2 * n1 <= 2^20 (I <= 256 at n1 = 2048) and
+ * returns VIA_ERR_INVALID_ARGUMENT above that. The first call on a device looks
+ * up the array's device address; make it before any stream capture. Calls that
+ * overlap on the GPU race on the shared array. This entry point has no
+ * counterpart in the reference.
+ */
+via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
+
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t via_kernel_launches(void);
 

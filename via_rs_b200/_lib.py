@@ -64,6 +64,8 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_server_reserve.restype = ctypes.c_int
     L.via_server_reserve.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+    L.via_first_dim_scan_static.restype = ctypes.c_int
+    L.via_first_dim_scan_static.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_kernel_launches.restype = ctypes.c_uint64
     L.via_kernel_launches.argtypes = []
     _lib = L

@@ -16,6 +16,15 @@ struct ApiError : std::runtime_error {
 unsigned long long g_kernel_launches = 0;
 static thread_local std::string g_last_error;
 
+// Scratch for via_first_dim_scan_static: the split selection vectors (one uint2
+// per residue) live in this file-scope device array instead of memory the call
+// allocates. Every device that loads the library holds it (8 MiB) until exit.
+constexpr u64 STATIC_SCAN_SCRATCH = 1ull << 20;  // uint2 entries: I * 2 * n1 <= 2^20
+static __device__ __align__(256) uint2 g_scan_scratch[STATIC_SCAN_SCRATCH];
+// Device address of g_scan_scratch per device, resolved once with that device current.
+static std::mutex g_scan_scratch_mu;
+static uint2* g_scan_scratch_addr[128] = {nullptr};
+
 template <class F>
 static via_status guarded(F&& f) {
   try {
@@ -308,6 +317,42 @@ via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint6
     std::lock_guard<std::mutex> g(s->mu);
     first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
                    (cudaStream_t)stream, workspace_sel_split(*s), s->fd_variant);
+  });
+}
+
+// The FirstDim scan for callers that cannot allocate device memory: same kernel
+// and result as via_first_dim_scan_dev, but its split-selection scratch is the
+// static array above, so this call makes no allocation. The first call on a
+// device resolves the array's device address (cudaGetSymbolAddress); make that
+// first call before any stream capture. Every call shares the array: calls
+// whose work overlaps on the GPU race on it. Each call overwrites every entry it
+// later reads, so nothing has to start at zero.
+via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream) {
+  return guarded([&] {
+    if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    const via_params& p = s->prm;
+    const u64 need = p.num_rows * 2 * (u64)p.n1;
+    if (need > STATIC_SCAN_SCRATCH)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "via_first_dim_scan_static: num_rows * 2 * n1 = " + std::to_string(need) +
+                                                   " exceeds the static scratch of " +
+                                                   std::to_string(STATIC_SCAN_SCRATCH) + " entries");
+    int dev = 0;
+    VIA_CUDA(cudaGetDevice(&dev));
+    if (dev < 0 || dev >= 128) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    uint2* scratch = nullptr;
+    {
+      std::lock_guard<std::mutex> g(g_scan_scratch_mu);
+      if (!g_scan_scratch_addr[dev]) {
+        void* addr = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&addr, g_scan_scratch);
+        if (e != cudaSuccess)
+          throw CudaError(102, std::string("cudaGetSymbolAddress(g_scan_scratch): ") + cudaGetErrorString(e));
+        g_scan_scratch_addr[dev] = static_cast<uint2*>(addr);
+      }
+      scratch = g_scan_scratch_addr[dev];
+    }
+    first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
+                   (cudaStream_t)stream, scratch, s->fd_variant);
   });
 }
 
