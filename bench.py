@@ -4,8 +4,9 @@
 Workload (one step = one answer of one query): the paper VIA-C preset
 (n1=2048, n2=512, q1 two 37/38-bit primes, q2 34-bit) over a 1 GiB database of
 4-bit records laid out I=2^8 x J=2^12 (the reference's docs/params.html Table 4
-dimensions for 1 GiB). The prepared database is 16 GiB in HBM (one u64 residue
-per eval slot), far larger than L2, so every step streams it from DRAM.
+dimensions for 1 GiB). The prepared database is 10 GiB in HBM (five byte planes
+per eval-form residue, the operand layout of the tensor-core scan), far larger
+than L2, so every step streams it from DRAM.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -32,11 +33,15 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "answers/s and DB GB/s scanned, batched vs plain, 1 GiB DB; p50/p99 answer ms"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_first_dim_ntt launch on
-# the I=256, J=256 case (1.082155 GB + 5.650176 MB), scaled by the 16x more
-# database cells of the I=256, J=4096 workload (profiles/first_dim_scan.md).
-SCAN_TRAFFIC_BYTES_SMALL = 1.082155e9 + 5.650176e6
-SCAN_TRAFFIC_CELLS_SMALL = 256 * 256
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one scan launch on a
+# smaller case, per database cell (None until captured for the current kernel).
+SCAN_TRAFFIC_BYTES_PER_CELL = None
+
+
+def prepared_db_bytes(prm):
+    """Bytes of the byte-plane database: rows padded to 64, columns to 128."""
+    ru = lambda v, a: (v + a - 1) // a * a
+    return ru(prm.num_rows, 64) * ru(prm.num_cols, 128) * prm.n1 * 5
 
 
 def parse():
@@ -186,8 +191,8 @@ def config_dict(prm):
     return {"workload": f"paper VIA-C answer, {gib:g} GiB DB (I={prm.num_rows}, J={prm.num_cols}, n1={prm.n1}), "
                         "one query per step",
             "preset": "paper (q1=137438822401*274810798081, q2=17175674881, q3=8380417, q4=4096, p=16)",
-            "db_raw_bytes": prm.capacity * prm.n_rec // 2, "db_prepared_bytes": prm.num_rows * prm.num_cols * prm.n1 * 8,
-            "l2": f"inputs larger than L2: the {prm.num_rows * prm.num_cols * prm.n1 * 8 / (1 << 30):g} GiB prepared DB "
+            "db_raw_bytes": prm.capacity * prm.n_rec // 2, "db_prepared_bytes": prepared_db_bytes(prm),
+            "l2": f"inputs larger than L2: the {prepared_db_bytes(prm) / (1 << 30):g} GiB prepared DB "
                   "is streamed every step"}
 
 
@@ -257,7 +262,7 @@ def gpu_arm(args, prm):
         elapsed = float(t.item())
     n_answers = args.steps * world
     value = n_answers / elapsed
-    db_bytes = prm.num_rows * prm.num_cols * prm.n1 * 8
+    db_bytes = prepared_db_bytes(prm)
 
     # ---- e2e: the reference-facing host-buffer call, copies inside the region.
     for _ in range(2):
@@ -343,10 +348,11 @@ def gpu_arm(args, prm):
             "plain": {"answers_s": value, "db_gbs": value * db_bytes / 1e9, "db_raw_gbs": value * (1 << 30) / 1e9,
                       "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
             "batched": batched,
-            "roofline": {"bound": "hbm", "kernel": "k_first_dim_ntt (FirstDim scan)", "achieved": achieved,
+            "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": SCAN_TRAFFIC_BYTES_SMALL * prm.num_rows * prm.num_cols / SCAN_TRAFFIC_CELLS_SMALL, "launch_ms": scan_s * 1e3,
-                         "algorithmic_bytes": scan_bytes},
+                         "traffic": (SCAN_TRAFFIC_BYTES_PER_CELL * prm.num_rows * prm.num_cols
+                                     if SCAN_TRAFFIC_BYTES_PER_CELL else None),
+                         "launch_ms": scan_s * 1e3, "algorithmic_bytes": scan_bytes},
             "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
                     "d2h_bytes_per_step": int(2 * prm.n2 * 8)},
             "gpu_launches": int(launches),

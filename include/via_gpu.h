@@ -174,6 +174,15 @@ via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* 
 via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
 
 /*
+ * The scans of n_queries independent queries in one pass over the database
+ * (the T first_dim calls of answer_batch, srv/batch.rs:139-150, sharing the
+ * scan): `sel_eval` holds [n_queries][I][2][n1] eval-form selection RLWEs,
+ * `out_eval` receives [n_queries][J][2][n1]. Allocates its scratch per call.
+ */
+via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, uint64_t n_queries,
+                                       uint64_t* out_eval, void* stream);
+
+/*
  * Runs the answer up to `stage` and copies that stage's output, in coefficient
  * form, to the host buffer `out` (for stage-by-stage parity checks):
  *   1 cascade RLWEs [n_lwe][2][nl][n1]      (query_decomp.rs:76-78)

@@ -131,3 +131,52 @@ def test_answer_many_equals_single_answers(oracle, preset):
             cm, cb = cpu.answer(qs[k])
             assert np.array_equal(gm[k], cm) and np.array_equal(gb[k], cb), (nq, k)
             assert np.array_equal(client.recover(gm[k], gb[k]), records[i])
+
+
+def _scan_setup(oracle, rows, cols, seed):
+    prm = paper_preset(rows, cols)
+    rng = np.random.default_rng(seed)
+    records = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client = oracle.Client(prm, b"scan-%d" % seed)
+    gpu = Server.setup(prm, PublicKeys(client.cascade_key, client.conv_key, client.rsk), records)
+    return prm, rng, gpu
+
+
+@pytest.mark.parametrize("nq", [2, 9, 24, 25, 64])
+def test_scan_many_equals_single_scans(oracle, nq):
+    """The shared scan of nq queries (grouped tensor-core tiles, several column
+    tiles and row chunks) equals nq single-query scans, which are pinned to the
+    oracle above."""
+    import torch
+
+    prm, rng, gpu = _scan_setup(oracle, 128, 256, 5)
+    sel = rng.integers(0, prm.q2, size=(nq, prm.num_rows * 2 * prm.n1), dtype=np.uint64)
+    if nq == 25:
+        sel[3] = prm.q2 - 1  # largest exact sums in one column of the batch
+    d_sel = torch.from_numpy(sel.view(np.int64)).cuda()
+    d_many = torch.empty(nq * prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
+    gpu.scan_many_dev(d_sel.data_ptr(), nq, d_many.data_ptr())
+    torch.cuda.synchronize()
+    d_one = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
+    many = d_many.view(nq, -1)
+    for b in range(nq):
+        gpu.scan_dev(d_sel[b].data_ptr(), d_one.data_ptr())
+        torch.cuda.synchronize()
+        assert torch.equal(many[b], d_one), f"query {b} of {nq}"
+
+
+def test_first_dim_matches_oracle_multi_tile(oracle):
+    """Two 64-row chunks and two 128-column tiles of the byte-plane database
+    against the oracle's first_dim."""
+    import torch
+
+    prm = paper_preset(128, 256)
+    rng = np.random.default_rng(12)
+    records = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client, gpu, cpu = _setup(oracle, prm, records, b"fd-multi")
+    sel = rng.integers(0, prm.q2, size=prm.num_rows * 2 * prm.n1, dtype=np.uint64)
+    want = cpu.first_dim(sel)
+    d_in = torch.from_numpy(sel.view(np.int64)).cuda()
+    d_out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
+    gpu.first_dim_dev(d_in.data_ptr(), d_out.data_ptr())
+    assert np.array_equal(d_out.cpu().numpy().view(np.uint64), want)

@@ -55,6 +55,9 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_void_p, ctypes.c_void_p]
     L.via_first_dim_scan_dev.restype = ctypes.c_int
     L.via_first_dim_scan_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_first_dim_scan_many_dev.restype = ctypes.c_int
+    L.via_first_dim_scan_many_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                              ctypes.c_void_p]
     L.via_debug_stage.restype = ctypes.c_int
     L.via_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, ctypes.c_int, _u64p, ctypes.c_uint64]
     L.via_server_answer_many.restype = ctypes.c_int

@@ -1,0 +1,532 @@
+// The FirstDim scan as a tcgen05 integer GEMM (crates/via-server/src/first_dim.rs:94-184).
+//
+// One persistent CTA per SM walks work units (t, c-tile): for every database
+// column tile jt it streams the (t, jt) byte planes chunk by chunk (64 rows of
+// the reduction at a time) together with the matching chunk of the split
+// selection, issues the byte-product MMAs into a TMEM accumulator, and an
+// epilogue folds the accumulator columns into residues mod q2.
+//
+// Warp roles (320 threads): warp 0 lane 0 issues the bulk copies, warp 1
+// allocates TMEM and its lane 0 issues the MMAs, warps 2..9 read TMEM and write
+// the outputs. Every wait is bounded in time; when one runs out the CTA raises
+// an error word and leaves its loops instead of waiting on.
+//
+// Accumulator placement. The selection chunk stacks the five byte limbs of the
+// N columns of a c-tile as rows l*N + c of the MMA's N dimension. The MMA of
+// database limb k writes TMEM columns starting at k*S:
+//  * grouped tiles (S = N, N a multiple of 16): column k*N + l*N + c collects
+//    every product with k + l = g in column g*N + c, nine groups per output;
+//  * the single-query tile (N = 2, S = 16): five disjoint regions of 16
+//    columns, product (k, l, c) in column 16k + 2l + c.
+#include <algorithm>
+
+#include "fd_tc.cuh"
+
+namespace via {
+namespace {
+
+constexpr int EPI_WARPS = 8;
+constexpr int FD_THREADS = 64 + 32 * EPI_WARPS;
+constexpr int ZERO_TILE = 256 * 32;  // zero operand for clearing grouped accumulators
+constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
+constexpr unsigned WAIT_SPINS = 1u << 26;
+
+struct KParams {
+  const uint8_t* db;
+  const uint8_t* sel;
+  u64* out;
+  int* err;
+  int n, J, n_jt, n_kc, n_ct, N, Np, nq;
+  int stages, grouped, acc_stride, nacc, tmem_cols;
+  DevMod m;
+};
+
+__device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ void mbar_init(u64* bar, u32 count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
+}
+__device__ __forceinline__ void mbar_expect_tx(u64* bar, u32 bytes) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void mbar_arrive(u64* bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(u64* bar, u32 parity) {
+  u32 ok;
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+      "selp.u32 %0, 1, 0, p;\n\t}\n"
+      : "=r"(ok)
+      : "r"(smem_addr(bar)), "r"(parity)
+      : "memory");
+  return ok != 0;
+}
+__device__ __forceinline__ unsigned long long global_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+  return t;
+}
+// Waits for the phase of `parity` to complete. Gives up (false) after WAIT_NS,
+// after WAIT_SPINS polls, or, when `honor_abort`, once another role of the CTA
+// has aborted.
+__device__ bool mbar_wait(u64* bar, u32 parity, volatile int* abort_flag, bool honor_abort = true) {
+  if (mbar_try_wait(bar, parity)) return true;
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 1; it < WAIT_SPINS; ++it) {
+    if (mbar_try_wait(bar, parity)) return true;
+    if ((it & 31) == 0) {
+      if (honor_abort && *abort_flag) return false;
+      if (global_ns() - t0 > WAIT_NS) return false;
+    }
+  }
+  return false;
+}
+
+__device__ __forceinline__ void bulk_g2s(void* dst, const void* src, u32 bytes, u64* bar) {
+  asm volatile(
+      "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(smem_addr(dst)),
+      "l"(src), "r"(bytes), "r"(smem_addr(bar))
+      : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// Shared-memory matrix descriptor, K-major without swizzle: 8-row x 16-byte
+// core matrices, `lbo` bytes between the two core matrices of a 32-byte K
+// slice, `sbo` bytes between 8-row groups.
+__device__ __forceinline__ u64 smem_desc(u32 addr, u32 lbo, u32 sbo) {
+  return (u64)((addr >> 4) & 0x3FFF) | ((u64)((lbo >> 4) & 0x3FFF) << 16) | ((u64)((sbo >> 4) & 0x3FFF) << 32) |
+         (1ull << 46);
+}
+
+// kind::i8 instruction descriptor: unsigned A and B, K-major, S32 accumulator, M = 128.
+__device__ __forceinline__ u32 idesc_u8(int n) { return (2u << 4) | ((u32)(n >> 3) << 17) | ((u32)(128 >> 4) << 24); }
+
+__device__ __forceinline__ void mma_u8(u32 d_tmem, u64 adesc, u64 bdesc, u32 idesc, u32 accumulate) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::i8 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d_tmem),
+      "l"(adesc), "l"(bdesc), "r"(idesc), "r"(accumulate)
+      : "memory");
+}
+__device__ __forceinline__ void mma_commit(u64* bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_addr(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tmem_ld8(u32 taddr, u32 (&r)[8]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
+               : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_ld16(u32 taddr, u32 (&r)[16]) {
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, %15}, "
+      "[%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]), "=r"(r[8]),
+        "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+}
+__device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+// Orders later uses of r after the wait above (the loads' results are only
+// defined once tcgen05.wait::ld has returned).
+template <int K>
+__device__ __forceinline__ void pin(u32 (&r)[K]) {
+#pragma unroll
+  for (int x = 0; x < K; ++x) asm volatile("" : "+r"(r[x]));
+}
+
+// sum_g v_g 2^{8g} mod q for nine group sums v_g < 2^31.
+__device__ __forceinline__ u64 fold9(const u32 (&v)[9], const DevMod& m) {
+  const u64 lo = (u64)v[0] + ((u64)v[1] << 8) + ((u64)v[2] << 16) + ((u64)v[3] << 24);
+  const u64 hi = (u64)v[4] + ((u64)v[5] << 8) + ((u64)v[6] << 16) + ((u64)v[7] << 24) + ((u64)v[8] << 32);
+  // lo + hi * 2^32 as 128 bits.
+  const u64 s_lo = lo + (hi << 32);
+  const u64 s_hi = (hi >> 32) + (s_lo < lo ? 1 : 0);
+  return reduce128(s_hi, s_lo, m);
+}
+
+__global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
+  extern __shared__ __align__(1024) uint8_t smem[];
+  const int stage_bytes = FD_CHUNK + P.Np * FD_KC;
+  uint8_t* zero_tile = smem + (size_t)P.stages * stage_bytes;
+  u64* full = reinterpret_cast<u64*>(zero_tile + ZERO_TILE);
+  u64* empty = full + P.stages;
+  u64* acc_full = empty + P.stages;
+  u64* acc_empty = acc_full + 2;
+  u64* drain = acc_empty + 2;
+  u32* tmem_slot = reinterpret_cast<u32*>(drain + 1);
+  volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
+
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  if (threadIdx.x == 0) {
+    for (int s = 0; s < P.stages; ++s) {
+      mbar_init(full + s, 1);
+      mbar_init(empty + s, 1);
+    }
+    for (int a = 0; a < 2; ++a) {
+      mbar_init(acc_full + a, 1);
+      mbar_init(acc_empty + a, EPI_WARPS * 32);
+    }
+    mbar_init(drain, 1);
+    *abort_flag = 0;
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+  }
+  for (int x = threadIdx.x; x < ZERO_TILE / 16; x += blockDim.x)
+    reinterpret_cast<uint4*>(zero_tile)[x] = make_uint4(0, 0, 0, 0);
+  asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+  if (warp == 1) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_addr(tmem_slot)),
+                 "r"((u32)P.tmem_cols)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const u32 tmem = *tmem_slot;
+
+  const int units = P.n * P.n_ct;
+  const u32 sel_chunk = (u32)P.Np * FD_KC;
+
+  if (warp == 0) {
+    if (lane == 0) {
+      // ---- Producer: bulk copies of (database chunk, selection chunk) per stage.
+      int s = 0;
+      u32 ph = 0;
+      u32 armed = 0, armed_par = 0;  // per stage: armed at least once; parity of its last armed phase
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
+        const int t = u / P.n_ct, ct = u % P.n_ct;
+        const uint8_t* selu = P.sel + ((size_t)t * P.n_ct + ct) * P.n_kc * sel_chunk;
+        const uint8_t* dbt = P.db + (size_t)t * P.n_jt * P.n_kc * FD_CHUNK;
+        for (int jt = 0; ok && jt < P.n_jt; ++jt)
+          for (int kc = 0; kc < P.n_kc; ++kc) {
+            if (!mbar_wait(empty + s, ph ^ 1, abort_flag)) {
+              ok = false;
+              break;
+            }
+            uint8_t* dst = smem + (size_t)s * stage_bytes;
+            mbar_expect_tx(full + s, FD_CHUNK + sel_chunk);
+            bulk_g2s(dst, dbt + ((size_t)jt * P.n_kc + kc) * FD_CHUNK, FD_CHUNK, full + s);
+            bulk_g2s(dst + FD_CHUNK, selu + (size_t)kc * sel_chunk, sel_chunk, full + s);
+            armed |= 1u << s;
+            armed_par = (armed_par & ~(1u << s)) | (ph << s);
+            if (++s == P.stages) {
+              s = 0;
+              ph ^= 1;
+            }
+          }
+      }
+      if (!ok) {
+        atomicOr(P.err, 1);
+        *abort_flag = 1;
+      }
+      // Every copy this CTA started lands before the CTA can exit: the last
+      // phase armed on each stage completes (at once on the normal path).
+      for (int k = 0; k < P.stages; ++k)
+        if ((armed >> k) & 1)
+          if (!mbar_wait(full + k, (armed_par >> k) & 1, abort_flag, false)) atomicOr(P.err, 1);
+    }
+  } else if (warp == 1) {
+    if (lane == 0) {
+      // ---- MMA issuer.
+      int s = 0, a = 0;
+      u32 ph = 0, aph = 0;
+      bool ok = true;
+      const u32 lbo_a = (FD_MT / 8) * 128, lbo_b = (u32)(P.Np / 8) * 128;
+      const u32 idesc = idesc_u8(P.Np);
+      const u32 zero_addr = smem_addr(zero_tile);
+      for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
+        for (int jt = 0; ok && jt < P.n_jt; ++jt) {
+          if (!mbar_wait(acc_empty + a, aph ^ 1, abort_flag)) {
+            ok = false;
+            break;
+          }
+          tc_fence_after();
+          const u32 dacc = tmem + (u32)(a * P.acc_stride);
+          if (P.grouped)  // columns [4N, 9N) start at zero; [0, 5N) are set by the first limb-0 product.
+            mma_u8(dacc + 4 * P.N, smem_desc(zero_addr, lbo_a, 128), smem_desc(zero_addr, lbo_b, 128), idesc, 0);
+          for (int kc = 0; kc < P.n_kc; ++kc) {
+            if (!mbar_wait(full + s, ph, abort_flag)) {
+              ok = false;
+              break;
+            }
+            tc_fence_after();
+            const u32 sa = smem_addr(smem + (size_t)s * stage_bytes);
+            const u32 sb = sa + FD_CHUNK;
+#pragma unroll
+            for (int ks = 0; ks < FD_KC / 32; ++ks) {
+#pragma unroll
+              for (int k = 0; k < FD_LIMBS; ++k) {
+                const u64 ad = smem_desc(sa + k * (FD_MT * FD_KC) + ks * 2 * lbo_a, lbo_a, 128);
+                const u64 bd = smem_desc(sb + ks * 2 * lbo_b, lbo_b, 128);
+                const u32 col = P.grouped ? (u32)(k * P.N) : (u32)(16 * k);
+                const u32 accum = (kc == 0 && ks == 0) ? (P.grouped ? (k > 0) : 0u) : 1u;
+                mma_u8(dacc + col, ad, bd, idesc, accum);
+              }
+            }
+            mma_commit(empty + s);  // frees the stage once these MMAs have read it
+            if (++s == P.stages) {
+              s = 0;
+              ph ^= 1;
+            }
+          }
+          if (!ok) break;
+          mma_commit(acc_full + a);
+          if (++a == P.nacc) {
+            a = 0;
+            aph ^= 1;
+          }
+        }
+      }
+      if (!ok) {
+        atomicOr(P.err, 2);
+        *abort_flag = 1;
+      }
+      // Every MMA issued above completes before TMEM is released.
+      mma_commit(drain);
+      if (!mbar_wait(drain, 0, abort_flag, false)) atomicOr(P.err, 2);
+    }
+  } else {
+    // ---- Epilogue: TMEM -> residues mod q2 -> out[b][j][mb][t].
+    const int ew = warp - 2, quad = warp & 3, half = ew >> 2;
+    const int row = quad * 32 + lane;
+    int a = 0;
+    u32 aph = 0;
+    bool ok = true;
+    for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
+      const int t = u / P.n_ct, ct = u % P.n_ct;
+      for (int jt = 0; jt < P.n_jt; ++jt) {
+        // Warp-uniform: the TMEM loads below are .sync.aligned.
+        if (!__all_sync(0xffffffffu, mbar_wait(acc_full + a, aph, abort_flag))) {
+          ok = false;
+          break;
+        }
+        tc_fence_after();
+        const u32 tb = tmem + (u32)(a * P.acc_stride) + ((u32)(quad * 32) << 16);
+        const int j = jt * FD_MT + row;
+        const bool jok = j < P.J;
+        if (P.grouped) {
+          const int c_lo = half * (P.N / 2), c_hi = c_lo + P.N / 2;
+          for (int c0 = c_lo; c0 < c_hi; c0 += 8) {
+            u32 v[9][8];
+#pragma unroll
+            for (int g = 0; g < 9; ++g) tmem_ld8(tb + (u32)(g * P.N + c0), v[g]);
+            tmem_wait_ld();
+#pragma unroll
+            for (int g = 0; g < 9; ++g) pin(v[g]);
+#pragma unroll
+            for (int x = 0; x < 8; ++x) {
+              const int cg = ct * P.N + c0 + x;
+              if (jok && cg < 2 * P.nq) {
+                u32 w[9];
+#pragma unroll
+                for (int g = 0; g < 9; ++g) w[g] = v[g][x];
+                const int b = cg >> 1, mb = cg & 1;
+                P.out[(((size_t)b * P.J + j) * 2 + mb) * P.n + t] = fold9(w, P.m);
+              }
+            }
+          }
+        } else {
+          u32 r[FD_LIMBS][16];
+#pragma unroll
+          for (int k = 0; k < FD_LIMBS; ++k) tmem_ld16(tb + (u32)(16 * k), r[k]);
+          tmem_wait_ld();
+#pragma unroll
+          for (int k = 0; k < FD_LIMBS; ++k) pin(r[k]);
+          // N = 2: half 0 writes the mask column, half 1 the body.
+          u32 w0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, w1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
+#pragma unroll
+          for (int k = 0; k < FD_LIMBS; ++k)
+#pragma unroll
+            for (int l = 0; l < FD_LIMBS; ++l) {
+              w0[k + l] += r[k][2 * l];
+              w1[k + l] += r[k][2 * l + 1];
+            }
+          u32 w[9];
+#pragma unroll
+          for (int g = 0; g < 9; ++g) w[g] = half ? w1[g] : w0[g];
+          if (jok) P.out[((size_t)j * 2 + half) * P.n + t] = fold9(w, P.m);
+        }
+        tc_fence_before();
+        mbar_arrive(acc_empty + a);
+        if (++a == P.nacc) {
+          a = 0;
+          aph ^= 1;
+        }
+      }
+    }
+    if (!ok) {
+      atomicOr(P.err, 4);
+      *abort_flag = 1;
+    }
+  }
+
+  tc_fence_before();
+  __syncthreads();
+  if (warp == 1) {
+    tc_fence_after();
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"((u32)P.tmem_cols)
+                 : "memory");
+  }
+}
+
+// Split selection: [t][ct][kc][Np x 64 bytes, core-matrix order], row l*N + c
+// holding byte l of column c (query b = cg/2, mask or body = cg%2) of the
+// c-tile. One thread per (t, ct, c, 16 consecutive rows i).
+__global__ void k_fd_split(const u64* __restrict__ sel, int nq, int I, int n, int n_k16, int n_kc, int n_ct, int N,
+                           int Np, uint8_t* __restrict__ out) {
+  const long total = (long)n * n_ct * N * n_k16;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= total) return;
+  const int t = (int)(gid % n);
+  long r = gid / n;
+  const int k16 = (int)(r % n_k16);
+  r /= n_k16;
+  const int c = (int)(r % N);
+  const int ct = (int)(r / N);
+  const int cg = ct * N + c;
+  const bool valid = cg < 2 * nq;
+  const int b = cg >> 1, mb = cg & 1;
+  u32 w[FD_LIMBS][4];
+#pragma unroll
+  for (int l = 0; l < FD_LIMBS; ++l) w[l][0] = w[l][1] = w[l][2] = w[l][3] = 0;
+#pragma unroll
+  for (int x = 0; x < 16; ++x) {
+    const int i = k16 * 16 + x;
+    if (valid && i < I) {
+      const u64 v = sel[(((size_t)b * I + i) * 2 + mb) * n + t];
+#pragma unroll
+      for (int l = 0; l < FD_LIMBS; ++l) w[l][x >> 2] |= (u32)((v >> (8 * l)) & 0xFF) << (8 * (x & 3));
+    }
+  }
+  const int kc = k16 / (FD_KC / 16), kk = k16 % (FD_KC / 16);
+  uint8_t* base = out + (((size_t)t * n_ct + ct) * n_kc + kc) * ((size_t)Np * FD_KC);
+#pragma unroll
+  for (int l = 0; l < FD_LIMBS; ++l) {
+    const int rr = l * N + c;
+    *reinterpret_cast<uint4*>(base + ((size_t)kk * (Np / 8) + rr / 8) * 128 + (rr % 8) * 16) =
+        make_uint4(w[l][0], w[l][1], w[l][2], w[l][3]);
+  }
+}
+
+// Database rows [i0, i0 + 16) (u64 [16][J][n]) -> byte planes. One thread per (t, j).
+__global__ void k_fd_planes(const u64* __restrict__ stage, int i0, int I, int J, int n, int n_jt, int n_kc,
+                            uint8_t* __restrict__ planes) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= (long)J * n) return;
+  const int t = (int)(gid % n), j = (int)(gid / n);
+  u32 w[FD_LIMBS][4];
+#pragma unroll
+  for (int l = 0; l < FD_LIMBS; ++l) w[l][0] = w[l][1] = w[l][2] = w[l][3] = 0;
+#pragma unroll
+  for (int x = 0; x < 16; ++x) {
+    if (i0 + x < I) {
+      const u64 v = stage[((size_t)x * J + j) * n + t];
+#pragma unroll
+      for (int l = 0; l < FD_LIMBS; ++l) w[l][x >> 2] |= (u32)((v >> (8 * l)) & 0xFF) << (8 * (x & 3));
+    }
+  }
+  const int kc = i0 / FD_KC, kk = (i0 % FD_KC) / 16;
+  const int jt = j / FD_MT, r = j % FD_MT;
+  uint8_t* base = planes + (((size_t)t * n_jt + jt) * n_kc + kc) * FD_CHUNK;
+#pragma unroll
+  for (int l = 0; l < FD_LIMBS; ++l)
+    *reinterpret_cast<uint4*>(base + (size_t)l * FD_MT * FD_KC + ((size_t)kk * (FD_MT / 8) + r / 8) * 128 +
+                              (r % 8) * 16) = make_uint4(w[l][0], w[l][1], w[l][2], w[l][3]);
+}
+
+struct Tiling {
+  int grouped, N, Np, n_ct, stages, acc_stride, nacc, tmem_cols;
+  size_t smem;
+};
+
+Tiling tiling(int nq) {
+  Tiling T{};
+  int acc_cols;
+  if (nq == 1) {
+    T.grouped = 0;
+    T.N = 2;
+    T.Np = 16;
+    T.n_ct = 1;
+    T.stages = 4;
+    acc_cols = 16 * FD_LIMBS;
+  } else {
+    T.grouped = 1;
+    T.n_ct = (2 * nq + 47) / 48;
+    T.N = fd_round_up((2 * nq + T.n_ct - 1) / T.n_ct, 16);
+    T.Np = FD_LIMBS * T.N;
+    T.stages = 3;
+    acc_cols = 9 * T.N;
+  }
+  T.acc_stride = fd_round_up(acc_cols, 32);
+  T.nacc = 2 * T.acc_stride <= 512 ? 2 : 1;
+  int cols = T.nacc * T.acc_stride, p2 = 32;
+  while (p2 < cols) p2 <<= 1;
+  T.tmem_cols = p2;
+  T.smem = (size_t)T.stages * (FD_CHUNK + (size_t)T.Np * FD_KC) + ZERO_TILE + 256;
+  return T;
+}
+
+}  // namespace
+
+size_t fd_planes_bytes(int I, int J, int n) {
+  return (size_t)fd_round_up(I, FD_KC) * fd_round_up(J, FD_MT) * n * FD_LIMBS;
+}
+
+bool fd_supported(int I, int n, u64 q) { return I >= 1 && I <= 4096 && n >= 1 && q < (1ull << 40); }
+
+void fd_rows_to_planes(const u64* stage, int i0, const FdPlan& p, uint8_t* planes, cudaStream_t st) {
+  const long total = (long)p.J * p.n;
+  k_fd_planes<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(stage, i0, p.I, p.J, p.n, p.J_pad / FD_MT,
+                                                              p.I_pad / FD_KC, planes);
+  VIA_LAUNCHED();
+}
+
+size_t fd_sel_bytes(const FdPlan& p, int nq) {
+  Tiling T = tiling(nq);
+  return (size_t)p.n * T.n_ct * (size_t)T.Np * p.I_pad;
+}
+
+void fd_prepare_device() {
+  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+}
+
+void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st) {
+  const Tiling T = tiling(nq);
+  const int n_k16 = p.I_pad / 16, n_kc = p.I_pad / FD_KC;
+  const long total = (long)p.n * T.n_ct * T.N * n_k16;
+  k_fd_split<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(sel_eval, nq, p.I, p.n, n_k16, n_kc, T.n_ct, T.N, T.Np,
+                                                              scratch);
+  VIA_LAUNCHED();
+  KParams K;
+  K.db = p.planes;
+  K.sel = scratch;
+  K.out = out_eval;
+  K.err = p.err;
+  K.n = p.n;
+  K.J = p.J;
+  K.n_jt = p.J_pad / FD_MT;
+  K.n_kc = n_kc;
+  K.n_ct = T.n_ct;
+  K.N = T.N;
+  K.Np = T.Np;
+  K.nq = nq;
+  K.stages = T.stages;
+  K.grouped = T.grouped;
+  K.acc_stride = T.acc_stride;
+  K.nacc = T.nacc;
+  K.tmem_cols = T.tmem_cols;
+  K.m = p.m;
+  const int units = p.n * T.n_ct;
+  const int grid = std::min(units, p.grid);
+  k_fd_tc<<<grid, FD_THREADS, T.smem, st>>>(K);
+  VIA_LAUNCHED();
+}
+
+}  // namespace via

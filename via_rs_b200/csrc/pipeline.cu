@@ -13,6 +13,7 @@
 // multiply-accumulate against the eval-form key (k_mac) -> inverse NTT. Linear
 // steps between products are done in whichever domain saves transforms; since
 // the NTT is exact, the coefficient-form results equal the reference's.
+#include <algorithm>
 #include <cmath>
 #include <cstring>
 
@@ -365,7 +366,7 @@ struct Workspace {
   // DMux.
   DevBuf dm_a, dm_b, dm_digits, dm_ext;
   // FirstDim / CMux.
-  DevBuf sel, sel_split, fd_out, cm_diff, cm_digits, cm_ext, cm_b;
+  DevBuf sel, sel_bytes, fd_out, cm_diff, cm_digits, cm_ext, cm_b;
   // CRot / RespComp.
   DevBuf cr_ct, cr_diff, cr_digits, cr_ext, rs_ct3, rs_mproj, rs_bproj, rs_digits, rs_gp, rs_acc;
   Gadget g_ck, g_dmux, g_cmux, g_rsk;
@@ -380,36 +381,17 @@ struct Workspace {
 
 void WorkspaceDeleter::operator()(Workspace* w) const { delete w; }
 void workspace_destroy(Server& s) { s.ws.reset(); }
-uint2* workspace_sel_split(Server& s) { return reinterpret_cast<uint2*>(s.ws->sel_split.p); }
+uint8_t* workspace_sel_bytes(Server& s) { return reinterpret_cast<uint8_t*>(s.ws->sel_bytes.p); }
 
-// Times each FirstDim column tile on the prepared database and keeps the fastest.
-void autotune_first_dim(Server& s) {
+void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st) {
   const via_params& p = s.prm;
-  if (!s.r2.ntt || !first_dim_split_ok((int)p.num_rows, (int)p.n1, p.q2)) return;
-  Workspace& w = *s.ws;
-  VIA_CUDA(cudaMemsetAsync(w.sel.p, 0, w.sel.n * 8, s.stream));
-  cudaEvent_t e0, e1;
-  VIA_CUDA(cudaEventCreate(&e0));
-  VIA_CUDA(cudaEventCreate(&e1));
-  float best = 1e30f;
-  for (int v = 0; v < first_dim_variants(); ++v) {
-    first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], true, s.stream,
-                   workspace_sel_split(s), v);
-    VIA_CUDA(cudaEventRecord(e0, s.stream));
-    for (int r = 0; r < 2; ++r)
-      first_dim_eval(s.db.p, w.sel.p, w.fd_out.p, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], true,
-                     s.stream, workspace_sel_split(s), v);
-    VIA_CUDA(cudaEventRecord(e1, s.stream));
-    VIA_CUDA(cudaEventSynchronize(e1));
-    float ms = 0;
-    VIA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
-    if (ms < best) {
-      best = ms;
-      s.fd_variant = v;
-    }
+  if (s.tensor_fd()) {
+    fd_scan(s.fd, sel_eval, out_eval, nq, scratch, st);
+    return;
   }
-  cudaEventDestroy(e0);
-  cudaEventDestroy(e1);
+  for (int q = 0; q < nq; ++q)
+    first_dim_schoolbook(s.db.p, sel_eval + (size_t)q * p.num_rows * 2 * p.n1, out_eval + (size_t)q * p.num_cols * 2 * p.n1,
+                         (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], st);
 }
 
 void workspace_create(Server& s, int bmax) {
@@ -438,7 +420,11 @@ void workspace_create(Server& s, int bmax) {
   w->dm_digits.alloc(B * std::max(1L, I / 2) * 2 * L * nl * n1);
   w->dm_ext.alloc(B * std::max(1L, I / 2) * 2 * nl * n1);
   w->sel.alloc(B * I * 2 * n1);
-  w->sel_split.alloc(B * I * 2 * n1);  // uint2 per residue
+  if (s.tensor_fd()) {
+    size_t bytes = 0;  // the split selection grows with the batch; size it for every batch up to B
+    for (int nq = 1; nq <= B; ++nq) bytes = std::max(bytes, fd_sel_bytes(s.fd, nq));
+    w->sel_bytes.alloc((bytes + 7) / 8);
+  }
   w->fd_out.alloc(B * J * 2 * n1);
   w->cm_diff.alloc(B * std::max(1L, J / 2) * 2 * n1);
   w->cm_digits.alloc(B * std::max(1L, J / 2) * 2 * L * n1);
@@ -675,8 +661,7 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
   // ---- Step 4: FirstDim (answer.rs:204-205), one pass over the database for
   // the whole batch; the columns stay in the eval domain.
   to_eval(s.r2, w.sel.p, n1, B * 2 * I, st);
-  first_dim_eval_batch(s.db.p, w.sel.p, w.fd_out.p, nq, (int)I, (int)J, n1, s.r2.m[0], s.r2.ntt, st,
-                       workspace_sel_split(s), s.fd_variant);
+  first_dim_queries(s, w.sel.p, w.fd_out.p, nq, workspace_sel_bytes(s), st);
   if (stop_stage == 5) {
     copy_out(w.fd_out.p, (size_t)J * 2 * n1);
     from_eval(s.r2, dump, n1, 2 * J, st);

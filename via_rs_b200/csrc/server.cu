@@ -16,14 +16,15 @@ struct ApiError : std::runtime_error {
 unsigned long long g_kernel_launches = 0;
 static thread_local std::string g_last_error;
 
-// Scratch for via_first_dim_scan_static: the split selection vectors (one uint2
-// per residue) live in this file-scope device array instead of memory the call
-// allocates. Every device that loads the library holds it (8 MiB) until exit.
-constexpr u64 STATIC_SCAN_SCRATCH = 1ull << 20;  // uint2 entries: I * 2 * n1 <= 2^20
-static __device__ __align__(256) uint2 g_scan_scratch[STATIC_SCAN_SCRATCH];
+// Scratch for via_first_dim_scan_static: the split selection vectors (five
+// byte planes padded to 16 rows per query and row, 16 * I * n1 bytes) live in
+// this file-scope device array instead of memory the call allocates. Every
+// device that loads the library holds it (8 MiB) until exit.
+constexpr u64 STATIC_SCAN_SCRATCH = 8ull << 20;  // bytes: 16 * I * n1 <= 2^23, i.e. I * 2 * n1 <= 2^20
+static __device__ __align__(256) uint4 g_scan_scratch[STATIC_SCAN_SCRATCH / 16];
 // Device address of g_scan_scratch per device, resolved once with that device current.
 static std::mutex g_scan_scratch_mu;
-static uint2* g_scan_scratch_addr[128] = {nullptr};
+static uint8_t* g_scan_scratch_addr[128] = {nullptr};
 
 template <class F>
 static via_status guarded(F&& f) {
@@ -61,6 +62,17 @@ void DevBuf::free() {
   if (p) cudaFree(p);
   p = nullptr;
   n = 0;
+}
+
+// Raises VIA_ERR_TIMEOUT once the FirstDim scan has reported that one of its
+// bounded waits ran out (the word stays set for the handle's lifetime).
+static void check_device_flags(Server& s, cudaStream_t st) {
+  if (!s.fd_err.p) return;
+  int flag = 0;
+  VIA_CUDA(cudaMemcpyAsync(&flag, s.fd_err.p, sizeof(int), cudaMemcpyDeviceToHost, st));
+  VIA_CUDA(cudaStreamSynchronize(st));
+  if (flag)
+    throw ApiError(VIA_ERR_TIMEOUT, "FirstDim scan: a bounded device wait ran out (flag " + std::to_string(flag) + ")");
 }
 
 int ilog2(u64 v) { return v <= 1 ? 0 : 63 - __builtin_clzll(v); }
@@ -202,27 +214,56 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
   s.r3 = make_ring(s, p.n2, p.q3, 0);
   s.r4 = make_ring(s, p.n2, p.q4, 0);
 
-  // Prepared database.
-  s.db.alloc(I * J * p.n1);
-  VIA_CUDA(cudaMemsetAsync(s.db.p, 0, s.db.n * 8, s.stream));
+  // Prepared database (setup_db.rs:39-75, prepared_db.rs:57-85): records are
+  // encoded into cells, lifted p -> q2 and transformed, 16 rows at a time.
   size_t rec_bytes = fmt == VIA_RECORDS_U64 ? (size_t)p.n_rec * 8 : (size_t)p.n_rec / 2;
-  const size_t chunk_records = std::max<size_t>(1, ((size_t)256 << 20) / rec_bytes);
+  if (s.r2.ntt && !fd_supported((int)I, (int)p.n1, p.q2))
+    throw ApiError(VIA_ERR_INVALID_ARGUMENT, "FirstDim needs num_rows <= 4096 and q2 < 2^40 for NTT-friendly q2");
+  const bool tensor = s.r2.ntt;
+  const u64 rows_per_pass = tensor ? 16 : I;
+  DevBuf cells;  // u64 cells of one pass: [rows_per_pass][J][n1]
+  if (tensor) {
+    s.fd.I = (int)I;
+    s.fd.J = (int)J;
+    s.fd.n = (int)p.n1;
+    s.fd.I_pad = fd_round_up((int)I, FD_KC);
+    s.fd.J_pad = fd_round_up((int)J, FD_MT);
+    s.fd.m = s.r2.m[0];
+    VIA_CUDA(cudaDeviceGetAttribute(&s.fd.grid, cudaDevAttrMultiProcessorCount, s.device));
+    fd_prepare_device();
+    s.planes.alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1) / 8);
+    VIA_CUDA(cudaMemsetAsync(s.planes.p, 0, s.planes.n * 8, s.stream));
+    s.fd_err.alloc(1);
+    VIA_CUDA(cudaMemsetAsync(s.fd_err.p, 0, 8, s.stream));
+    s.fd.err = reinterpret_cast<int*>(s.fd_err.p);
+    cells.alloc(rows_per_pass * J * p.n1);
+  } else {
+    s.db.alloc(I * J * p.n1);
+  }
+  u64* cell_buf = tensor ? cells.p : s.db.p;
   void* stage = nullptr;
-  if (n_records) VIA_CUDA(cudaMalloc(&stage, std::min<size_t>(chunk_records, I * J) * rec_bytes));
+  if (n_records) VIA_CUDA(cudaMalloc(&stage, (size_t)std::min<u64>(rows_per_pass * J, n_records) * rec_bytes));
   try {
-    for (int k = 0; k < d; ++k) {
-      u64 lo = (u64)k * I * J;
-      if (lo >= n_records) break;
-      u64 hi = std::min<u64>(n_records, lo + I * J);
-      for (u64 c0 = lo; c0 < hi; c0 += chunk_records) {
-        u64 c1 = std::min<u64>(hi, c0 + chunk_records);
-        const char* src = (const char*)records + (size_t)c0 * rec_bytes;
-        VIA_CUDA(cudaMemcpyAsync(stage, src, (size_t)(c1 - c0) * rec_bytes, cudaMemcpyHostToDevice, s.stream));
-        u64 threads = (c1 - c0) * p.n_rec;
-        k_encode_slot<<<(unsigned)((threads + 255) / 256), 256, 0, s.stream>>>(stage, fmt, c1 - c0, c0 - lo, k,
-                                                                               p.n1, d, p.n_rec, p.p, s.db.p);
+    for (u64 i0 = 0; i0 < I; i0 += rows_per_pass) {
+      const u64 rows = std::min<u64>(rows_per_pass, I - i0);
+      VIA_CUDA(cudaMemsetAsync(cell_buf, 0, rows_per_pass * J * p.n1 * 8, s.stream));
+      for (int k = 0; k < d; ++k) {
+        // Records of slot k whose cells lie in rows [i0, i0 + rows).
+        const u64 lo = (u64)k * I * J + i0 * J;
+        const u64 hi = std::min<u64>(n_records, lo + rows * J);
+        if (lo >= hi) continue;
+        const char* src = (const char*)records + (size_t)lo * rec_bytes;
+        VIA_CUDA(cudaMemcpyAsync(stage, src, (size_t)(hi - lo) * rec_bytes, cudaMemcpyHostToDevice, s.stream));
+        u64 threads = (hi - lo) * p.n_rec;
+        k_encode_slot<<<(unsigned)((threads + 255) / 256), 256, 0, s.stream>>>(stage, fmt, hi - lo, 0, k, p.n1, d,
+                                                                               p.n_rec, p.p, cell_buf);
         VIA_LAUNCHED();
         VIA_CUDA(cudaStreamSynchronize(s.stream));
+      }
+      if (s.r2.ntt) ntt_forward(cell_buf, p.n1, 1, (long)(rows * J), s.r2.t[0], s.r2.t[0], s.stream);
+      if (tensor) {
+        s.fd.planes = reinterpret_cast<const uint8_t*>(s.planes.p);
+        fd_rows_to_planes(cell_buf, (int)i0, s.fd, reinterpret_cast<uint8_t*>(s.planes.p), s.stream);
       }
     }
   } catch (...) {
@@ -230,7 +271,8 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     throw;
   }
   if (stage) cudaFree(stage);
-  if (s.r2.ntt) ntt_forward(s.db.p, p.n1, 1, (long)(I * J), s.r2.t[0], s.r2.t[0], s.stream);
+  VIA_CUDA(cudaStreamSynchronize(s.stream));
+  cells.free();
 
   // Keys.
   if (keys) {
@@ -244,7 +286,6 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     transform_keys(s);
   }
   workspace_create(s, 1);
-  autotune_first_dim(s);
   VIA_CUDA(cudaStreamSynchronize(s.stream));
 }
 
@@ -284,10 +325,10 @@ via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* 
     VIA_CUDA(cudaMemcpyAsync(sel.p, switched, sel.n * 8, cudaMemcpyDeviceToDevice, st));
     if (s->r2.ntt) ntt_forward(sel.p, p.n1, 1, (long)(2 * p.num_rows), s->r2.t[0], s->r2.t[0], st);
     std::lock_guard<std::mutex> g(s->mu);
-    first_dim_eval(s->db.p, sel.p, out, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt, st,
-                   workspace_sel_split(*s), s->fd_variant);
+    first_dim_queries(*s, sel.p, out, 1, workspace_sel_bytes(*s), st);
     if (s->r2.ntt) ntt_inverse(out, p.n1, 1, (long)(2 * p.num_cols), s->r2.t[0], s->r2.t[0], st);
     VIA_CUDA(cudaStreamSynchronize(st));
+    check_device_flags(*s, st);
   });
 }
 
@@ -313,10 +354,22 @@ via_status via_server_answer_dev(via_server* s, const uint64_t* query, uint64_t 
 via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream) {
   return guarded([&] {
     if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
-    const via_params& p = s->prm;
     std::lock_guard<std::mutex> g(s->mu);
-    first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
-                   (cudaStream_t)stream, workspace_sel_split(*s), s->fd_variant);
+    first_dim_queries(*s, sel_eval, out_eval, 1, workspace_sel_bytes(*s), (cudaStream_t)stream);
+  });
+}
+
+via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, uint64_t n_queries,
+                                       uint64_t* out_eval, void* stream) {
+  return guarded([&] {
+    if (!s || !sel_eval || !out_eval || n_queries == 0 || n_queries > 4096)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument or batch size outside 1..4096");
+    DevBuf scratch;
+    if (s->tensor_fd()) scratch.alloc((fd_sel_bytes(s->fd, (int)n_queries) + 7) / 8);
+    std::lock_guard<std::mutex> g(s->mu);
+    first_dim_queries(*s, sel_eval, out_eval, (int)n_queries, reinterpret_cast<uint8_t*>(scratch.p),
+                      (cudaStream_t)stream);
+    VIA_CUDA(cudaStreamSynchronize((cudaStream_t)stream));  // scratch is freed on return
   });
 }
 
@@ -325,21 +378,22 @@ via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint6
 // static array above, so this call makes no allocation. The first call on a
 // device resolves the array's device address (cudaGetSymbolAddress); make that
 // first call before any stream capture. Every call shares the array: calls
-// whose work overlaps on the GPU race on it. Each call overwrites every entry it
-// later reads, so nothing has to start at zero.
+// whose work overlaps on the GPU race on it. Each call writes every scratch byte
+// that reaches its result (the padding rows it leaves alone only feed
+// accumulator columns that are never read), so nothing has to start at zero.
 via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream) {
   return guarded([&] {
     if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
     const via_params& p = s->prm;
-    const u64 need = p.num_rows * 2 * (u64)p.n1;
+    const u64 need = s->tensor_fd() ? fd_sel_bytes(s->fd, 1) : 0;
     if (need > STATIC_SCAN_SCRATCH)
-      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "via_first_dim_scan_static: num_rows * 2 * n1 = " + std::to_string(need) +
-                                                   " exceeds the static scratch of " +
-                                                   std::to_string(STATIC_SCAN_SCRATCH) + " entries");
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "via_first_dim_scan_static: the split selection needs " +
+                                                   std::to_string(need) + " bytes (16 * num_rows * n1), more than the "
+                                                   "static scratch of " + std::to_string(STATIC_SCAN_SCRATCH) + " bytes");
     int dev = 0;
     VIA_CUDA(cudaGetDevice(&dev));
     if (dev < 0 || dev >= 128) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "device ordinal out of range");
-    uint2* scratch = nullptr;
+    uint8_t* scratch = nullptr;
     {
       std::lock_guard<std::mutex> g(g_scan_scratch_mu);
       if (!g_scan_scratch_addr[dev]) {
@@ -347,12 +401,12 @@ via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, ui
         cudaError_t e = cudaGetSymbolAddress(&addr, g_scan_scratch);
         if (e != cudaSuccess)
           throw CudaError(102, std::string("cudaGetSymbolAddress(g_scan_scratch): ") + cudaGetErrorString(e));
-        g_scan_scratch_addr[dev] = static_cast<uint2*>(addr);
+        g_scan_scratch_addr[dev] = static_cast<uint8_t*>(addr);
       }
       scratch = g_scan_scratch_addr[dev];
     }
-    first_dim_eval(s->db.p, sel_eval, out_eval, (int)p.num_rows, (int)p.num_cols, (int)p.n1, s->r2.m[0], s->r2.ntt,
-                   (cudaStream_t)stream, scratch, s->fd_variant);
+    (void)p;
+    first_dim_queries(*s, sel_eval, out_eval, 1, scratch, (cudaStream_t)stream);
   });
 }
 
@@ -373,6 +427,7 @@ via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe,
     answer_device_stages(*s, dq.p, 1, dm.p, db.p, s->stream, stage, dout.p);
     VIA_CUDA(cudaMemcpyAsync(out, dout.p, sizes[stage] * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
+    check_device_flags(*s, s->stream);
   });
 }
 
@@ -435,6 +490,7 @@ via_status via_server_answer_many(via_server* s, const uint64_t* queries, uint64
     VIA_CUDA(cudaMemcpyAsync(out_bodies, workspace_answer_body(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToHost,
                              s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
+    check_device_flags(*s, s->stream);
   });
 }
 
@@ -457,6 +513,7 @@ via_status via_server_answer(via_server* s, const uint64_t* query, uint64_t n_lw
     VIA_CUDA(cudaMemcpyAsync(out_mask, workspace_answer_mask(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaMemcpyAsync(out_body, workspace_answer_body(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
+    check_device_flags(*s, s->stream);
   });
 }
 

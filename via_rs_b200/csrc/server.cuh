@@ -7,6 +7,7 @@
 
 #include "../../include/via_gpu.h"
 #include "common.cuh"
+#include "fd_tc.cuh"
 #include "ntt.cuh"
 
 namespace via {
@@ -48,15 +49,20 @@ struct Server {
   // Rings: q1 at n1 (1 or 2 limbs), q2 at n1, q3 at n1 and n2, q4 at n2.
   DevRing r1, r2, r3n1, r3, r4;
   std::vector<NttTableHost> tables;  // owners
-  // Prepared database: [I][J][n1] eval-form residues mod q2.
+  // Prepared database. NTT-friendly q2: byte planes for the tensor-core scan
+  // (fd_tc.cuh layout) in `planes`, described by `fd`. Otherwise (schoolbook
+  // rings): [I][J][n1] u64 residues in `db`.
   DevBuf db;
+  DevBuf planes;
+  FdPlan fd;
+  DevBuf fd_err;  // one device word the scan sets when a bounded wait runs out
   // Eval-form keys (crates/via-server/src/prepared_keys.rs:69-79).
   DevBuf cascade_eval;  // include/via_gpu.h cascade layout, each segment transformed
   DevBuf conv_eval;     // L_CK samples at (q1, n1)
   DevBuf rsk_eval;      // d RLevs at (q3, n2)
   std::unique_ptr<Workspace, WorkspaceDeleter> ws;
   std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
-  int fd_variant = 1;  // FirstDim column tile chosen at setup (autotuned)
+  bool tensor_fd() const { return fd.planes != nullptr; }
   ~Server();
 };
 
@@ -73,12 +79,13 @@ int ilog2(u64 v);
 void workspace_create(Server& s, int bmax);
 int workspace_batch(Server& s);
 void workspace_destroy(Server& s);
-uint2* workspace_sel_split(Server& s);
+uint8_t* workspace_sel_bytes(Server& s);
+// FirstDim of nq queries: sel_eval [nq][I][2][n1] -> out_eval [nq][J][2][n1] (eval at q2).
+void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st);
 u64* workspace_query(Server& s);
 u64* workspace_answer_mask(Server& s);
 u64* workspace_answer_body(Server& s);
 void answer_graph(Server& s, int nq, cudaStream_t st);
-void autotune_first_dim(Server& s);
 void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st);
 void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u64* d_body, cudaStream_t st,
                           int stop_stage, u64* dump);

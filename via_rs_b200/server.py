@@ -159,6 +159,16 @@ class Server:
         check(_lib.lib().via_first_dim_dev(self._h, ctypes.c_void_p(switched_ptr), ctypes.c_void_p(out_ptr),
                                            ctypes.c_void_p(stream)))
 
+    def scan_dev(self, sel_eval_ptr: int, out_eval_ptr: int, stream: int = 0) -> None:
+        """The FirstDim scan alone on eval-form device buffers (one query)."""
+        check(_lib.lib().via_first_dim_scan_dev(self._h, ctypes.c_void_p(sel_eval_ptr), ctypes.c_void_p(out_eval_ptr),
+                                                ctypes.c_void_p(stream)))
+
+    def scan_many_dev(self, sel_eval_ptr: int, n_queries: int, out_eval_ptr: int, stream: int = 0) -> None:
+        """The scans of n_queries queries in one pass over the database (eval form)."""
+        check(_lib.lib().via_first_dim_scan_many_dev(self._h, ctypes.c_void_p(sel_eval_ptr), n_queries,
+                                                     ctypes.c_void_p(out_eval_ptr), ctypes.c_void_p(stream)))
+
     def close(self) -> None:
         if self._h:
             _lib.lib().via_server_destroy(self._h)
