@@ -72,6 +72,7 @@ struct Gadget {
   u128 Q, halfQ;
   u64 half_base;
   u64 magic;      // floor(2^64 / B) for the 64-bit digit divisions
+  bool small;     // Q * (S + 1) < 2^53: one limb, and the scaling is exact in doubles
 };
 
 inline Gadget make_gadget(u64 base, int L, u128 Q) {
@@ -104,6 +105,7 @@ inline Gadget make_gadget(u64 base, int L, u128 Q) {
   g.dS_over_Q = dS / g.dQ;
   g.half_base = base / 2;
   g.magic = (u64)(((u128)1 << 64) / base);
+  g.small = Q < ((u128)1 << 53) && S < ((u128)1 << 53) && Q * (S + 1) < ((u128)1 << 53);
   return g;
 }
 
@@ -139,7 +141,22 @@ __host__ __device__ __forceinline__ u64 digits64(u64 u, int cnt, const Gadget& g
 // centred lift c (v <= Q/2 ? v : v - Q), then round(|c| B^L / Q) with c's sign
 // (gadget.rs:115-151). The balanced digits (gadget.rs:168-190) depend only on
 // this value mod B^L.
+// The scaled value for a `small` gadget (one limb, Q (S + 1) < 2^53): mag * S +
+// floor(Q/2) is an exact double, so one division and a +-1 fix give the exact
+// quotient. The result is below S < 2^53 and is the single digit chunk.
+__host__ __device__ __forceinline__ u64 gadget_scaled_small(u64 a0, const Gadget& g) {
+  const u64 Q = (u64)g.Q, hq = (u64)g.halfQ, S = (u64)g.S;
+  const bool neg = a0 > hq;
+  const u64 mag = neg ? Q - a0 : a0;
+  const u64 num = mag * S + hq;
+  u64 qe = (u64)((double)num / g.dQ);
+  for (int it = 0; it < 2 && qe * Q > num; ++it) --qe;
+  for (int it = 0; it < 2 && num - qe * Q >= Q; ++it) ++qe;
+  return (neg && qe != 0) ? S - qe : qe;
+}
+
 __host__ __device__ __forceinline__ u128 gadget_scaled(u64 a0, u64 a1, const DevRing& R, const Gadget& g) {
+  if (g.small) return (u128)gadget_scaled_small(a0, g);
   u128 v = R.nl == 2 ? crt2(a0, a1, R) : (u128)a0;
   bool neg = v > g.halfQ;
   u128 mag = neg ? g.Q - v : v;
@@ -177,6 +194,18 @@ __host__ __device__ __forceinline__ void gadget_chunks(u128 u, const Gadget& g, 
 // at k == c the high chunk takes over with the low chunk's carry.
 __host__ __device__ __forceinline__ i64 gadget_next_digit(u64& cur, u64 hi, int k, const Gadget& g) {
   if (k == g.c) cur = hi + cur;
+  u64 r;
+  u64 q = divB(cur, g, r);
+  if (r > g.half_base) {
+    cur = q + 1;
+    return (i64)r - (i64)g.base;
+  }
+  cur = q;
+  return (i64)r;
+}
+
+// Next balanced digit of a single-chunk (small) gadget.
+__host__ __device__ __forceinline__ i64 gadget_next_digit_small(u64& cur, const Gadget& g) {
   u64 r;
   u64 q = divB(cur, g, r);
   if (r > g.half_base) {

@@ -115,6 +115,29 @@ __device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const Ntt
   }
 }
 
+// Inverse transform (Gentleman-Sande, then the n^-1 scaling) of a segment whose
+// eval-form residues a thread holds in the layout NttPhase<LOGN,true,0>::index;
+// leaves the coefficients in the layout of the last inverse phase.
+template <int LOGN, int P = 0>
+__device__ __forceinline__ void ntt_inverse_regs(u64 (&e)[8], int tid, const NttTable& T, u64* ssm) {
+  using Ph = NttPhase<LOGN, true, P>;
+  constexpr int NPH = (LOGN + 2) / 3;
+  Ph::run(e, tid, T);
+  if constexpr (P + 1 < NPH) {
+    using Nx = NttPhase<LOGN, true, P + 1>;
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = ssm[Nx::index(v, tid)];
+    ntt_inverse_regs<LOGN, P + 1>(e, tid, T, ssm);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q);
+  }
+}
+
 // Builds tables for q (prime, 2*nmax | q-1). Returns valid=false otherwise.
 NttTableHost make_ntt_table(u64 q, int nmax);
 void free_ntt_table(NttTableHost& t);

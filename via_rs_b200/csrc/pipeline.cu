@@ -242,6 +242,56 @@ __global__ void k_cascade_reduce(const u64* __restrict__ P, int rank_in, int N, 
   }
 }
 
+// One cascade step's key switches and rank reduction in a single pass
+// (conv.rs:122-148): the digits D of the R input masks are transformed at the
+// input degree n_in, where the eval form of embed_at(d, 0) (d(X^2) of degree
+// 2 n_in) is d's own eval form with every slot repeated (slot t of the output
+// degree reads slot t/2). For every output mask j < R/2 and slot t:
+//   mask_out[j] = -(sum_s D[j][s] K_j[s].mask + D[j+R/2][s] K_{j+R/2}[s].mask)
+//   bsum        =   sum_idx sum_s D[idx][s] K_idx[s].body
+// D: [lwe][idx][L][nl][n_in]; keys: [idx][L][2][nl][n_out]; mask_out:
+// [lwe][R/2][nl][n_out]; bsum: [lwe][nl][n_out]. Block = TT slots x JJ output
+// masks (TT * JJ = 256); the JJ lanes' body partials are summed in shared memory.
+__global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, const u64* __restrict__ keys, int R,
+                                                     int n_in, int L, int TT, DevRing Rg, u64* __restrict__ mask_out,
+                                                     u64* __restrict__ bsum) {
+  __shared__ u64 part[256];
+  const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
+  const int JJ = 256 / TT;
+  const int tl = threadIdx.x % TT, jl = threadIdx.x / TT;
+  const int t = blockIdx.x * TT + tl;
+  const int l = blockIdx.y;
+  const long lwe = blockIdx.z;
+  const DevMod& m = Rg.m[l];
+  const long dper = (long)nl * n_in, kper = (long)nl * n_out;
+  const u64* Dw = D + lwe * R * L * dper + (long)l * n_in + (t >> 1);
+  const u64* Kl = keys + (long)l * n_out + t;
+  Acc128 ab{0, 0};
+  for (int j = jl; j < half; j += JJ) {
+    Acc128 am{0, 0};
+    const u64* d0 = Dw + (long)j * L * dper;
+    const u64* d1 = Dw + (long)(j + half) * L * dper;
+    const u64* k0 = Kl + (long)j * L * 2 * kper;
+    const u64* k1 = Kl + (long)(j + half) * L * 2 * kper;
+#pragma unroll 3
+    for (int s = 0; s < L; ++s) {
+      const u64 a = d0[s * dper], b = d1[s * dper];
+      mac128(am, a, k0[(2 * s) * kper]);
+      mac128(am, b, k1[(2 * s) * kper]);
+      mac128(ab, a, k0[(2 * s + 1) * kper]);
+      mac128(ab, b, k1[(2 * s + 1) * kper]);
+    }
+    mask_out[((lwe * half + j) * nl + l) * n_out + t] = negmod(reduce128(am.hi, am.lo, m), m.q);
+  }
+  part[threadIdx.x] = reduce128(ab.hi, ab.lo, m);
+  __syncthreads();
+  if (jl == 0) {
+    u64 acc = part[tl];
+    for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
+    bsum[(lwe * nl + l) * n_out + t] = acc;
+  }
+}
+
 // body_out[lwe] = embed_at(body_in[lwe], N_out, 0) - bsum[lwe] (coefficient form).
 __global__ void k_cascade_body(const u64* __restrict__ body_in, const u64* __restrict__ bsum, int n_in, int nl,
                                long nlwe, DevRing R, u64* __restrict__ body_out) {
@@ -510,11 +560,22 @@ static void query_decomp(Server& s, const u64* d_query, int nq, cudaStream_t st)
   for (int n_in = 1; n_in < n1; n_in <<= 1, ++k) {
     const int n_out = 2 * n_in, rank_in = n1 / n_in;
     const long polys = nlwe * rank_in;
-    gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), w.c_P.p,
-                   w.c_digits.p, st);
-    const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
-    k_cascade_reduce<<<blocks(items), 256, 0, st>>>(w.c_P.p, rank_in, n_out, nl, nlwe, R, mo, w.c_bsum.p);
-    VIA_LAUNCHED();
+    if (R.ntt) {
+      // Digits at the input degree; see k_cascade_mac for the repeated slots.
+      decompose(R, w.g_ck, mi, n_in, 1, polys, w.c_digits.p, st);
+      if (n_in > 1) to_eval(R, w.c_digits.p, n_in, polys * L * nl, st);
+      int jj = std::min(rank_in / 2, 8), tt = std::min(n_out, 256 / jj);
+      dim3 grid((unsigned)(n_out / tt), (unsigned)nl, (unsigned)nlwe);
+      k_cascade_mac<<<grid, 256, 0, st>>>(w.c_digits.p, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, R, mo,
+                                          w.c_bsum.p);
+      VIA_LAUNCHED();
+    } else {
+      gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), w.c_P.p,
+                     w.c_digits.p, st);
+      const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
+      k_cascade_reduce<<<blocks(items), 256, 0, st>>>(w.c_P.p, rank_in, n_out, nl, nlwe, R, mo, w.c_bsum.p);
+      VIA_LAUNCHED();
+    }
     from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
     from_eval(R, w.c_bsum.p, n_out, nlwe * nl, st);
     k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, w.c_bsum.p, n_in, nl, nlwe, R, bo);
@@ -542,6 +603,90 @@ static void external_products(const DevRing& R, const Gadget& g, KeySel rgsw, co
   // pair with the neg_s_m and m samples of the RGSW respectively.
   gadget_product(R, g, cts, n, 1, 2, count, rgsw, ext, digits, st);
   if (to_coeff) from_eval(R, ext, n, 2 * count * R.nl, st);
+}
+
+// One CMux of a tree level per CTA (mux.rs:75-84, 167-198; rgsw.rs:108-121),
+// single-limb ring of degree 2^LOGN with a small gadget (gadget_scaled_small),
+// 2^LOGN / 8 threads holding 8 residues each:
+//   diff = in[2o+1] - in[2o] (eval) -> inverse NTT -> balanced digits of the
+//   mask and body -> forward NTT of each digit polynomial -> products with the
+//   RGSW samples (mask digits with neg_s_m, body digits with m, digit k with
+//   sample L-1-k) -> out[o] = in[2o] + ext, eval form throughout.
+// cur: [count*2][2][n]; nxt: [count][2][n]; the RGSW of CMux o ([2L][2][n],
+// eval) is picked by `ks`. The digits never leave registers.
+template <int LOGN>
+__global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __restrict__ cur, u64* __restrict__ nxt,
+                                                                  KeySel ks, DevRing R, Gadget g) {
+  constexpr int n = 1 << LOGN;
+  using In0 = NttPhase<LOGN, true, 0>;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  using Fw0 = NttPhase<LOGN, false, 0>;
+  using FwL = NttPhase<LOGN, false, (LOGN + 2) / 3 - 1>;
+  __shared__ u64 ssm[n];
+  const int tid = threadIdx.x;
+  const long o = blockIdx.x;
+  const NttTable& T = R.t[0];
+  const DevMod& m = R.m[0];
+  const u64 q = m.q;
+  const u64* a = cur + (2 * o) * 2 * n;
+  const u64* b = a + 2 * n;
+  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
+  const int L = g.L;
+  Acc128 am[8], ab[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) am[v] = ab[v] = Acc128{0, 0};
+  for (int p = 0; p < 2; ++p) {  // 0: mask digits (neg_s_m rows), 1: body digits (m rows)
+    u64 e[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const int x = In0::index(v, tid);
+      e[v] = submod(b[p * n + x], a[p * n + x], q);
+    }
+    ntt_inverse_regs<LOGN>(e, tid, T, ssm);
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) ssm[InL::index(v, tid)] = e[v];
+    __syncthreads();
+    u64 dcur[8];
+#pragma unroll
+    for (int v = 0; v < 8; ++v) dcur[v] = gadget_scaled_small(ssm[Fw0::index(v, tid)], g);
+    for (int k = 0; k < L; ++k) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit_small(dcur[v], g), m);
+      ntt_forward_regs<LOGN>(e, tid, T, ssm);
+      const u64* Km = K + (long)(2 * (p * L + L - 1 - k)) * n;
+      const u64* Kb = Km + n;
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        const int x = FwL::index(v, tid);
+        mac128(am[v], e[v], Km[x]);
+        mac128(ab[v], e[v], Kb[x]);
+      }
+    }
+  }
+  u64* out = nxt + o * 2 * n;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    const int x = FwL::index(v, tid);
+    out[x] = addmod(a[x], reduce128(am[v].hi, am[v].lo, m), q);
+    out[n + x] = addmod(a[n + x], reduce128(ab[v].hi, ab[v].lo, m), q);
+  }
+}
+
+// CMux level o < count: fused kernel when the ring has one NTT limb of a
+// supported degree and a small gadget, else diff -> external product -> add.
+static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
+  return R.ntt && R.nl == 1 && g.small && (R.n == 2048 || R.n == 1024 || R.n == 512);
+}
+
+static void cmux_fused(const DevRing& R, const Gadget& g, const u64* cur, u64* nxt, KeySel ks, long count,
+                       cudaStream_t st) {
+  switch (R.n) {
+    case 2048: k_cmux_fused<11><<<(unsigned)count, 256, 0, st>>>(cur, nxt, ks, R, g); break;
+    case 1024: k_cmux_fused<10><<<(unsigned)count, 128, 0, st>>>(cur, nxt, ks, R, g); break;
+    default: k_cmux_fused<9><<<(unsigned)count, 64, 0, st>>>(cur, nxt, ks, R, g); break;
+  }
+  VIA_LAUNCHED();
 }
 
 // CRot diff for nq RLWEs: rot = -(X^k * ct), diff = rot - ct.
@@ -673,13 +818,18 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
   u64* cur = w.fd_out.p;
   for (int i = 0; i < nc; ++i) {
     const long half = (J >> i) / 2;  // CMuxes per query at this level
+    KeySel bit{w.rgsw_q2.p + (nd + i) * rgsw2, half, B, w.nbits * rgsw2};
+    u64* nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
+    if (cmux_fused_ok(s.r2, w.g_cmux)) {
+      cmux_fused(s.r2, w.g_cmux, cur, nxt, bit, B * half, st);
+      cur = nxt;
+      continue;
+    }
     k_rlwe_addsub<<<blocks(B * half * 2 * n1), 256, 0, st>>>(w.cm_diff.p, cur + 2 * n1, 2, cur, 2, -1, B * half, n1, 1,
                                                              s.r2);
     VIA_LAUNCHED();
     from_eval(s.r2, w.cm_diff.p, n1, B * 2 * half, st);
-    KeySel bit{w.rgsw_q2.p + (nd + i) * rgsw2, half, B, w.nbits * rgsw2};
     external_products(s.r2, w.g_cmux, bit, w.cm_diff.p, B * half, w.cm_digits.p, w.cm_ext.p, false, st);
-    u64* nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
     k_rlwe_addsub<<<blocks(B * half * 2 * n1), 256, 0, st>>>(nxt, cur, 2, w.cm_ext.p, 1, +1, B * half, n1, 1, s.r2);
     VIA_LAUNCHED();
     cur = nxt;
