@@ -114,7 +114,8 @@ constexpr int NTT_THREADS = 256;
 // sub-blocks u; a thread owns 8 >> r consecutive sub-blocks.
 // ---------------------------------------------------------------------------
 template <int LOGN, bool INV, int P>
-__device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* ssm, bool active) {
+__device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* sm, int sbase,
+                                           bool active) {
   using Ph = NttPhase<LOGN, INV, P>;
   constexpr int NPH = (LOGN + 2) / 3;
   if (P == 0) {
@@ -123,14 +124,13 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
   } else {
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) e[v] = ssm[Ph::index(v, tid)];
+    for (int v = 0; v < 8; ++v) e[v] = sm[swz(sbase + Ph::index(v, tid))];
   }
   Ph::run(e, tid, T);
   if constexpr (P == NPH - 1) {
-    if (INV) {
 #pragma unroll
-      for (int v = 0; v < 8; ++v) e[v] = mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q);
-    }
+    for (int v = 0; v < 8; ++v)
+      e[v] = INV ? mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q) : ntt_canonical(e[v], T);
     if (active) {
 #pragma unroll
       for (int v = 0; v < 8; ++v) g[Ph::index(v, tid)] = e[v];
@@ -138,8 +138,8 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
   } else {
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
-    ntt_phases<LOGN, INV, P + 1>(e, tid, T, g, ssm, active);
+    for (int v = 0; v < 8; ++v) sm[swz(sbase + Ph::index(v, tid))] = e[v];
+    ntt_phases<LOGN, INV, P + 1>(e, tid, T, g, sm, sbase, active);
   }
 }
 
@@ -156,7 +156,7 @@ __global__ void __launch_bounds__(NTT_THREADS) k_ntt_reg(u64* __restrict__ data,
   const bool active = seg < segments;
   const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
   u64 e[8];
-  ntt_phases<LOGN, INV, 0>(e, tid, T, data + seg * n, sm + seg_local * n, active);
+  ntt_phases<LOGN, INV, 0>(e, tid, T, data + seg * n, sm, seg_local * n, active);
 }
 
 // n = 2 and 4: one thread per segment, all in registers.

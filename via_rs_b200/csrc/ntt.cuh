@@ -33,6 +33,16 @@ struct NttTableHost {
   bool valid = false;
 };
 
+// Shoup product without the final correction: a * w mod q in [0, 2q) for any
+// a < 2^64 (w < q, ws = floor(w * 2^64 / q)).
+__device__ __forceinline__ u64 shoup_lazy(u64 a, u64 w, u64 ws, u64 q) { return a * w - mulhi(a, ws) * q; }
+
+// Shared-memory slot of element x of an exchange: an XOR swizzle of the low
+// four bits by bits 4..9 keeps the strided phase layouts free of 8-byte bank
+// conflicts (at most two lanes of a half warp per bank). A bijection on every
+// aligned 16-element block, so segments of n >= 16 stay in place.
+__device__ __forceinline__ int swz(int x) { return x ^ (((x >> 4) ^ (x >> 5)) & 15); }
+
 // One phase (up to three butterfly stages) of the register-resident transform:
 // each thread holds 8 residues of a length-2^LOGN segment. Stage s of the
 // forward transform pairs (x, x + len_s), len_s = n >> (s+1), with twiddle
@@ -41,7 +51,17 @@ struct NttTableHost {
 // stages 3P..3P+R-1 and works on sub-blocks of 2^R residues x = base + k*STRIDE,
 // where STRIDE is the phase's smallest len and base = (u / STRIDE) *
 // (STRIDE << R) + u % STRIDE over the n >> R sub-blocks u; a thread owns
-// 8 >> R consecutive sub-blocks.
+// 8 >> R consecutive sub-blocks. A sub-block's butterflies at level lvl use
+// 2^lvl (forward) or 2^(R-1-lvl) (inverse) consecutive twiddles starting at
+// (u / STRIDE) times that count.
+//
+// Lazy residues (no conditional corrections inside a transform):
+//  * forward: t = a*w mod q in [0, 2q); (a, c) -> (a + t, a + 2q - t), so after
+//    s stages every residue is below (1 + 2s) q;
+//  * inverse: stage s inputs are below 2^s q; (a, c) -> (a + c, (a + 2^s q - c) w
+//    mod q in [0, 2q)).
+// Both stay far below 2^64 for q < 2^50 and n <= 4096; the transforms end
+// with one exact reduction (forward) or the n^-1 scaling (inverse).
 template <int LOGN, bool INV, int P>
 struct NttPhase {
   static constexpr int n = 1 << LOGN;
@@ -62,31 +82,38 @@ struct NttPhase {
 #pragma unroll
     for (int sub = 0; sub < NSUB; ++sub) {
       const int u = tid * NSUB + sub;
-      const int base = (u / STRIDE) * (STRIDE << R) + (u % STRIDE);
+      const int b0 = u / STRIDE;
 #pragma unroll
       for (int lvl = 0; lvl < R; ++lvl) {
         // forward: len = STRIDE << (R-1-lvl) (decreasing); inverse: STRIDE << lvl.
         const int hk = INV ? (1 << lvl) : (1 << (R - 1 - lvl));
         const int len = STRIDE * hk;
         const int m = n / (2 * len);
+        const int tw0 = m + (INV ? (b0 << (R - 1 - lvl)) : (b0 << lvl));
+        u64 w[4], ws[4];
+        const int ntw = INV ? (1 << (R - 1 - lvl)) : (1 << lvl);
+#pragma unroll
+        for (int j = 0; j < 4; ++j) {
+          if (j < ntw) {
+            w[j] = __ldg((INV ? T.ipsi : T.psi) + tw0 + j);
+            ws[j] = __ldg((INV ? T.ipsi_sh : T.psi_sh) + tw0 + j);
+          }
+        }
 #pragma unroll
         for (int k = 0; k < (1 << R); ++k) {
           if (k & hk) continue;
-          const int x = base + k * STRIDE;
-          const int grp = x / (2 * len);
+          const int j = INV ? (k >> (lvl + 1)) : (k >> (R - lvl));
           u64& a = e[sub * (1 << R) + k];
           u64& c = e[sub * (1 << R) + k + hk];
           if (!INV) {
-            const u64 w = __ldg(T.psi + m + grp), ws = __ldg(T.psi_sh + m + grp);
-            const u64 t = mul_shoup(c, w, ws, q);
+            const u64 t = shoup_lazy(c, w[j], ws[j], q);
             const u64 av = a;
-            a = addmod(av, t, q);
-            c = submod(av, t, q);
+            a = av + t;
+            c = av + 2 * q - t;
           } else {
-            const u64 w = __ldg(T.ipsi + m + grp), ws = __ldg(T.ipsi_sh + m + grp);
             const u64 av = a, cv = c;
-            a = addmod(av, cv, q);
-            c = mul_shoup(submod(av, cv, q), w, ws, q);
+            a = av + cv;
+            c = shoup_lazy(av + (q << (S0 + lvl)) - cv, w[j], ws[j], q);
           }
         }
       }
@@ -94,10 +121,15 @@ struct NttPhase {
   }
 };
 
+// Exact residue of a lazy forward output (below 2^64): Shoup by 1.
+__device__ __forceinline__ u64 ntt_canonical(u64 x, const NttTable& T) {
+  return mul_shoup(x, T.ninv[0], T.ninv_sh[0], T.q);
+}
 
 // Forward transform of a segment whose residues a thread already holds in the
-// phase-0 layout (NttPhase<LOGN,false,0>::index); leaves them in the layout of
-// the last phase. `ssm` is the segment's n-residue shared-memory exchange area.
+// phase-0 layout (NttPhase<LOGN,false,0>::index); leaves them (exact) in the
+// layout of the last phase. `ssm` is an n-residue shared-memory exchange area
+// of one segment, addressed through swz().
 template <int LOGN, int P = 0>
 __device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const NttTable& T, u64* ssm) {
   using Ph = NttPhase<LOGN, false, P>;
@@ -107,11 +139,14 @@ __device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const Ntt
     using Nx = NttPhase<LOGN, false, P + 1>;
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
+    for (int v = 0; v < 8; ++v) ssm[swz(Ph::index(v, tid))] = e[v];
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) e[v] = ssm[Nx::index(v, tid)];
+    for (int v = 0; v < 8; ++v) e[v] = ssm[swz(Nx::index(v, tid))];
     ntt_forward_regs<LOGN, P + 1>(e, tid, T, ssm);
+  } else {
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = ntt_canonical(e[v], T);
   }
 }
 
@@ -127,10 +162,10 @@ __device__ __forceinline__ void ntt_inverse_regs(u64 (&e)[8], int tid, const Ntt
     using Nx = NttPhase<LOGN, true, P + 1>;
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) ssm[Ph::index(v, tid)] = e[v];
+    for (int v = 0; v < 8; ++v) ssm[swz(Ph::index(v, tid))] = e[v];
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) e[v] = ssm[Nx::index(v, tid)];
+    for (int v = 0; v < 8; ++v) e[v] = ssm[swz(Nx::index(v, tid))];
     ntt_inverse_regs<LOGN, P + 1>(e, tid, T, ssm);
   } else {
 #pragma unroll

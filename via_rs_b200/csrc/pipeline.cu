@@ -645,11 +645,11 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __
     ntt_inverse_regs<LOGN>(e, tid, T, ssm);
     __syncthreads();
 #pragma unroll
-    for (int v = 0; v < 8; ++v) ssm[InL::index(v, tid)] = e[v];
+    for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
     __syncthreads();
     u64 dcur[8];
 #pragma unroll
-    for (int v = 0; v < 8; ++v) dcur[v] = gadget_scaled_small(ssm[Fw0::index(v, tid)], g);
+    for (int v = 0; v < 8; ++v) dcur[v] = gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
     for (int k = 0; k < L; ++k) {
 #pragma unroll
       for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit_small(dcur[v], g), m);
