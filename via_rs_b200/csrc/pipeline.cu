@@ -614,6 +614,21 @@ static void external_products(const DevRing& R, const Gadget& g, KeySel rgsw, co
 //   sample L-1-k) -> out[o] = in[2o] + ext, eval form throughout.
 // cur: [count*2][2][n]; nxt: [count][2][n]; the RGSW of CMux o ([2L][2][n],
 // eval) is picked by `ks`. The digits never leave registers.
+// Sum of products of residues below 2^40: each product's high word is below
+// 2^16, so up to 2^16 products fit a 32-bit high word (callers check q < 2^40).
+// Three registers instead of four.
+struct Acc96 {
+  u64 lo;
+  u32 hi;
+};
+__device__ __forceinline__ void mac96(Acc96& acc, u64 a, u64 b) {
+  const u64 pl = a * b;
+  const u32 ph = (u32)mulhi(a, b);
+  const u64 nl = acc.lo + pl;
+  acc.hi += ph + (nl < pl ? 1u : 0u);
+  acc.lo = nl;
+}
+
 template <int LOGN>
 __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __restrict__ cur, u64* __restrict__ nxt,
                                                                   KeySel ks, DevRing R, Gadget g) {
@@ -622,6 +637,9 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __
   using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
   using Fw0 = NttPhase<LOGN, false, 0>;
   using FwL = NttPhase<LOGN, false, (LOGN + 2) / 3 - 1>;
+  // The inverse's input and the forward's output layouts are 8 consecutive
+  // residues per thread (slot 8 tid + v), so those accesses are 16-byte vectors.
+  static_assert(In0::STRIDE == 1 && In0::R == 3 && FwL::STRIDE == 1, "contiguous end layouts");
   __shared__ u64 ssm[n];
   const int tid = threadIdx.x;
   const long o = blockIdx.x;
@@ -632,51 +650,71 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __
   const u64* b = a + 2 * n;
   const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
   const int L = g.L;
-  Acc128 am[8], ab[8];
+  Acc96 am[8], ab[8];
 #pragma unroll
-  for (int v = 0; v < 8; ++v) am[v] = ab[v] = Acc128{0, 0};
+  for (int v = 0; v < 8; ++v) am[v] = ab[v] = Acc96{0, 0};
   for (int p = 0; p < 2; ++p) {  // 0: mask digits (neg_s_m rows), 1: body digits (m rows)
     u64 e[8];
+    {
+      const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
+      const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
 #pragma unroll
-    for (int v = 0; v < 8; ++v) {
-      const int x = In0::index(v, tid);
-      e[v] = submod(b[p * n + x], a[p * n + x], q);
+      for (int h = 0; h < 4; ++h) {
+        const ulonglong2 x = bv[h], y = av[h];
+        e[2 * h] = submod(x.x, y.x, q);
+        e[2 * h + 1] = submod(x.y, y.y, q);
+      }
     }
     ntt_inverse_regs<LOGN>(e, tid, T, ssm);
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
     __syncthreads();
-    u64 dcur[8];
+    u32 dcur[8];  // scaled coefficients, below B^L < 2^32
 #pragma unroll
-    for (int v = 0; v < 8; ++v) dcur[v] = gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
+    for (int v = 0; v < 8; ++v) dcur[v] = (u32)gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
     for (int k = 0; k < L; ++k) {
 #pragma unroll
-      for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit_small(dcur[v], g), m);
-      ntt_forward_regs<LOGN>(e, tid, T, ssm);
-      const u64* Km = K + (long)(2 * (p * L + L - 1 - k)) * n;
-      const u64* Kb = Km + n;
-#pragma unroll
       for (int v = 0; v < 8; ++v) {
-        const int x = FwL::index(v, tid);
-        mac128(am[v], e[v], Km[x]);
-        mac128(ab[v], e[v], Kb[x]);
+        u64 c = dcur[v];
+        e[v] = lift_i64(gadget_next_digit_small(c, g), m);
+        dcur[v] = (u32)c;
+      }
+      ntt_forward_regs<LOGN>(e, tid, T, ssm);
+      const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * (p * L + L - 1 - k)) * n + 8 * tid);
+      const ulonglong2* Kb = Km + n / 2;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
+        mac96(am[2 * h], e[2 * h], km.x);
+        mac96(am[2 * h + 1], e[2 * h + 1], km.y);
+        mac96(ab[2 * h], e[2 * h], kb.x);
+        mac96(ab[2 * h + 1], e[2 * h + 1], kb.y);
       }
     }
   }
-  u64* out = nxt + o * 2 * n;
+  ulonglong2* outm = reinterpret_cast<ulonglong2*>(nxt + o * 2 * n + 8 * tid);
+  ulonglong2* outb = outm + n / 2;
+  const ulonglong2* am_in = reinterpret_cast<const ulonglong2*>(a + 8 * tid);
+  const ulonglong2* ab_in = am_in + n / 2;
 #pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    const int x = FwL::index(v, tid);
-    out[x] = addmod(a[x], reduce128(am[v].hi, am[v].lo, m), q);
-    out[n + x] = addmod(a[n + x], reduce128(ab[v].hi, ab[v].lo, m), q);
+  for (int h = 0; h < 4; ++h) {
+    const ulonglong2 xm = am_in[h], xb = ab_in[h];
+    ulonglong2 ym, yb;
+    ym.x = addmod(xm.x, reduce128(am[2 * h].hi, am[2 * h].lo, m), q);
+    ym.y = addmod(xm.y, reduce128(am[2 * h + 1].hi, am[2 * h + 1].lo, m), q);
+    yb.x = addmod(xb.x, reduce128(ab[2 * h].hi, ab[2 * h].lo, m), q);
+    yb.y = addmod(xb.y, reduce128(ab[2 * h + 1].hi, ab[2 * h + 1].lo, m), q);
+    outm[h] = ym;
+    outb[h] = yb;
   }
 }
 
 // CMux level o < count: fused kernel when the ring has one NTT limb of a
 // supported degree and a small gadget, else diff -> external product -> add.
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
-  return R.ntt && R.nl == 1 && g.small && (R.n == 2048 || R.n == 1024 || R.n == 512);
+  return R.ntt && R.nl == 1 && g.small && g.S < ((u128)1 << 32) && R.m[0].q < (1ull << 40) &&
+         (R.n == 2048 || R.n == 1024 || R.n == 512);
 }
 
 static void cmux_fused(const DevRing& R, const Gadget& g, const u64* cur, u64* nxt, KeySel ks, long count,
