@@ -33,9 +33,11 @@ ROOT = pathlib.Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
 METRIC = "answers/s and DB GB/s scanned, batched vs plain, 1 GiB DB; p50/p99 answer ms"
-# ncu dram__bytes_read.sum + dram__bytes_write.sum of one scan launch on a
-# smaller case, per database cell (None until captured for the current kernel).
-SCAN_TRAFFIC_BYTES_PER_CELL = None
+# ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_fd_tc launch on the
+# I=64, J=4096 case (2.749080 GB read, 174.374656 MB written): reads scale with the
+# database cells, writes with the columns (profiles/fd_tc_scan_paper.md).
+SCAN_READ_BYTES_PER_CELL = 2.749080e9 / (64 * 4096)
+SCAN_WRITE_BYTES_PER_COLUMN = 174.374656e6 / 4096
 
 
 def prepared_db_bytes(prm):
@@ -55,6 +57,8 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU oracle leg (for profiling)")
     ap.add_argument("--scan-launches", type=int, default=10)
     ap.add_argument("--batch", type=int, default=64, help="queries per shared-scan batch (0 = skip)")
+    ap.add_argument("--profile-batch", action="store_true",
+                    help="set up, answer one batch of --batch queries and exit (a short target for ncu)")
     return ap.parse_args()
 
 
@@ -231,6 +235,15 @@ def gpu_arm(args, prm):
         check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr()), prm.n_lwe,
                                       ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()), sptr))
 
+    if args.profile_batch:
+        B = max(1, args.batch)
+        qb = np.tile(query, B)
+        mb, bb = server.answer_many(qb.reshape(B, -1))
+        torch.cuda.synchronize()
+        print(json.dumps({"profile_batch": B, "answers": int(mb.shape[0])}), flush=True)
+        server.close()
+        return
+
     for _ in range(args.warmup):
         answer_dev()
     torch.cuda.synchronize()
@@ -350,8 +363,8 @@ def gpu_arm(args, prm):
             "batched": batched,
             "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
-                         "traffic": (SCAN_TRAFFIC_BYTES_PER_CELL * prm.num_rows * prm.num_cols
-                                     if SCAN_TRAFFIC_BYTES_PER_CELL else None),
+                         "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols
+                                     + SCAN_WRITE_BYTES_PER_COLUMN * prm.num_cols),
                          "launch_ms": scan_s * 1e3, "algorithmic_bytes": scan_bytes},
             "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
                     "d2h_bytes_per_step": int(2 * prm.n2 * 8)},
