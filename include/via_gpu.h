@@ -197,6 +197,23 @@ via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe,
                            uint64_t out_len);
 
 /*
+ * Server::answer_batch (VIA-B, crates/via-server/src/batch.rs:72-163): the
+ * server must have been set up with n_rec < n2; the batch size is then
+ * T = n2 / n_rec (the record-fit boundary T * n_rec = n2). `queries` holds T
+ * queries of n_lwe LWEs each, back to back (layout of via_server_answer); the
+ * single answer (n2 mask residues at q3, n2 body residues at q4) packs the T
+ * records, record t at plaintext slots t + (n2 / n_rec) * k. The T queries share
+ * one database scan, then the T CRot outputs are repacked (repack.rs) with the
+ * cascade key's last log2(n1 / n_rec) steps switched to q2, and RespComp runs
+ * once. VIA_ERR_DIM_MISMATCH when n_queries != T or the server is VIA-C only.
+ */
+via_status via_server_answer_batch(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                   uint64_t* out_mask, uint64_t* out_body);
+/* The same on device buffers, enqueued on `stream`. */
+via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                       uint64_t* out_mask, uint64_t* out_body, void* stream);
+
+/*
  * The FirstDim scan of via_first_dim_scan_dev for callers that cannot allocate
  * device memory: code that runs where cudaMalloc is not allowed or not wanted
  * (inside a region being captured into a CUDA graph, a host whose allocator is

@@ -106,6 +106,8 @@ struct OracleServer {
   Params prm;
   PreparedKeys keys;
   PreparedDb db;
+  CascadeKey cascade;                              // coefficient form, for the VIA-B repack keys
+  std::vector<std::vector<RlevEval>> repack_keys;  // derived on the first answer_batch
 };
 
 extern "C" {
@@ -195,6 +197,7 @@ void* vo_server_setup(const via_params* p, const uint64_t* cascade, const uint64
     src = rsk;
     for (int j = 0; j < prm.d(); ++j) pk.rsk.push_back(get_rlev(src, R3, prm.l_rsk));
     s->keys = prepare_keys(prm, pk);
+    s->cascade = pk.cascade;
     s->db = setup_db(prm, records, n_records, threads);
     out = s.release();
   });
@@ -210,6 +213,24 @@ int vo_server_answer(void* sv, const uint64_t* query, size_t n_lwe, uint64_t* ma
     answer(s->prm, q, s->keys, s->db, threads, m, b);
     std::memcpy(mask, m.data(), m.size() * 8);
     std::memcpy(body, b.data(), b.size() * 8);
+  });
+}
+
+// Server::answer_batch (srv/batch.rs:72-163): n_queries = T = n2 / n_rec queries
+// of n_lwe LWEs each, back to back; one answer.
+int vo_server_answer_batch(void* sv, const uint64_t* queries, size_t n_queries, size_t n_lwe, uint64_t* mask,
+                           uint64_t* body, int threads) {
+  return guarded([&] {
+    OracleServer* s = (OracleServer*)sv;
+    Ring R1 = s->prm.r1();
+    const size_t per = n_lwe * (size_t)R1.nl * (s->prm.n1 + 1);
+    std::vector<std::vector<Lwe>> qs;
+    for (size_t b = 0; b < n_queries; ++b) qs.push_back(get_query(queries + b * per, R1, n_lwe));
+    if (s->repack_keys.empty()) s->repack_keys = repack_keys(s->prm, s->cascade);
+    Poly m, bd;
+    answer_batch(s->prm, qs, s->keys, s->repack_keys, s->db, threads, m, bd);
+    std::memcpy(mask, m.data(), m.size() * 8);
+    std::memcpy(body, bd.data(), bd.size() * 8);
   });
 }
 

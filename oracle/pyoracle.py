@@ -43,6 +43,8 @@ def lib() -> ctypes.CDLL:
         L.vo_server_setup.restype = ctypes.c_void_p
         L.vo_server_setup.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p, _u64p, ctypes.c_size_t, ctypes.c_int]
         L.vo_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, _u64p, ctypes.c_int]
+        L.vo_server_answer_batch.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, _u64p,
+                                             ctypes.c_int]
         L.vo_server_answer_through_crot.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
         L.vo_server_first_dim.argtypes = [ctypes.c_void_p, _u64p, _u64p, ctypes.c_int]
         L.vo_server_free.argtypes = [ctypes.c_void_p]
@@ -113,6 +115,17 @@ class Client:
         _check(lib().vo_client_query(self._h, index, d, seed, len(seed), _ptr(out)))
         return out
 
+    def batch_query(self, indices, seed: bytes) -> np.ndarray:
+        """Client::batch_query (cli/client.rs:256-300): one query per index at d3 = n1 / n_rec."""
+        return np.stack([self.query(int(i), seed + b"-%d" % k) for k, i in enumerate(indices)])
+
+    def recover_batch(self, mask: np.ndarray, body: np.ndarray) -> list:
+        """Client::recover_batch (cli/client.rs:316-333, cli/batch.rs:35-58): record t is
+        project_at::<n_rec>(t) of the recovered degree-n2 plaintext."""
+        plain = self.recover(mask, body)
+        stride = self.prm.n2 // self.prm.n_rec
+        return [plain[t::stride] for t in range(stride)]
+
     def recover(self, mask: np.ndarray, body: np.ndarray) -> np.ndarray:
         out = np.zeros(self.prm.n2, dtype=np.uint64)
         _check(lib().vo_client_recover(self._h, _ptr(np.ascontiguousarray(mask, dtype=np.uint64)),
@@ -147,6 +160,18 @@ class Server:
         body = np.zeros(prm.n2, dtype=np.uint64)
         _check(lib().vo_server_answer(self._h, _ptr(q), q.size // prm.lwe_len, _ptr(mask), _ptr(body),
                                       self.threads))
+        return mask, body
+
+    def answer_batch(self, queries: np.ndarray):
+        """Server::answer_batch (srv/batch.rs:72-163): queries (T, n_lwe * lwe_len), one answer."""
+        prm = self.prm
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        if q.ndim != 2:
+            raise ValueError("queries must be (T, n_lwe * lwe_len)")
+        mask = np.zeros(prm.n2, dtype=np.uint64)
+        body = np.zeros(prm.n2, dtype=np.uint64)
+        _check(lib().vo_server_answer_batch(self._h, _ptr(q), q.shape[0], q.shape[1] // prm.lwe_len, _ptr(mask),
+                                            _ptr(body), self.threads))
         return mask, body
 
     def answer_through_crot(self, query: np.ndarray) -> np.ndarray:

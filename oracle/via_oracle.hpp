@@ -327,6 +327,19 @@ void resp_comp(const Params& prm, const Rlwe& ct_q2, const std::vector<RlevEval>
 void answer(const Params& prm, const std::vector<Lwe>& q, const PreparedKeys& k, const PreparedDb& db,
             int threads, Poly& mask_q3, Poly& body_q4);
 
+// ---------------------------------------------------------------------------
+// VIA-B — oracle_batch.cpp (conversion/extract.rs, conversion/repack.rs,
+// srv/batch.rs). The batch size is T = n2 / n_rec (the record-fit boundary).
+// ---------------------------------------------------------------------------
+Mlwe extr(const Ring& R, const Rlwe& ct, int g);
+Mlwe mlwes_to_mlwe(const Ring& Rout, const Ring& Rin, const Mlwe& a, const Mlwe& b, const std::vector<RlevEval>& keys,
+                   u64 base);
+std::vector<std::vector<RlevEval>> repack_keys(const Params& prm, const CascadeKey& ck);
+Rlwe repack(const Params& prm, const std::vector<Rlwe>& rotated, const std::vector<std::vector<RlevEval>>& keys);
+void answer_batch(const Params& prm, const std::vector<std::vector<Lwe>>& queries, const PreparedKeys& k,
+                  const std::vector<std::vector<RlevEval>>& rkeys, const PreparedDb& db, int threads, Poly& mask_q3,
+                  Poly& body_q4);
+
 // Stage timings (seconds) of the last answer() call on this thread.
 struct StageTimes {
   double t[8];

@@ -55,6 +55,12 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_void_p, ctypes.c_void_p]
     L.via_first_dim_scan_dev.restype = ctypes.c_int
     L.via_first_dim_scan_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_server_answer_batch.restype = ctypes.c_int
+    L.via_server_answer_batch.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                          ctypes.c_void_p, ctypes.c_void_p]
+    L.via_server_answer_batch_dev.restype = ctypes.c_int
+    L.via_server_answer_batch_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
+                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_first_dim_scan_many_dev.restype = ctypes.c_int
     L.via_first_dim_scan_many_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                               ctypes.c_void_p]

@@ -424,6 +424,7 @@ struct Workspace {
   DevBuf q_in, a_mask, a_body;
   std::vector<std::pair<int, cudaGraphExec_t>> graphs;  // one per batch size
   std::vector<std::pair<int, unsigned long long>> graph_kernels;
+  std::unique_ptr<struct RepackWs> repack;  // VIA-B buffers, made on the first batch answer
   ~Workspace() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
   }
@@ -788,6 +789,27 @@ __global__ void k_ring_switch_finish_batch(const u64* acc, const u64* body_proj,
   out_body[q * n2 + t] = r >= m4.q ? r - m4.q : r;
 }
 
+// Step 7, RespComp (resp_comp.rs:46-76), of B RLWEs at (q2, n1) in coefficient
+// form: q2 -> q3, ring switch n1 -> n2 with the RSK, body q3 -> q4.
+static void resp_comp(Server& s, const u64* ct_q2, long B, u64* d_mask, u64* d_body, cudaStream_t st) {
+  Workspace& w = *s.ws;
+  const via_params& p = s.prm;
+  const int n1 = p.n1, n2 = p.n2;
+  mod_switch(s.r2, ct_q2, s.r3n1, w.rs_ct3.p, B * 2, n1, st);
+  const int d = n1 / n2;
+  k_ring_switch_proj_batch<<<blocks(B * (d + 1) * n2), 256, 0, st>>>(w.rs_ct3.p, n1, n2, B, s.r3.m[0], w.rs_mproj.p,
+                                                                      w.rs_bproj.p);
+  VIA_LAUNCHED();
+  gadget_product(s.r3, w.g_rsk, w.rs_mproj.p, n2, 1, 1, B * d, keys_cyclic(s.rsk_eval.p, d), w.rs_gp.p,
+                 w.rs_digits.p, st);
+  k_ring_switch_sum_batch<<<blocks(B * 2 * n2), 256, 0, st>>>(w.rs_gp.p, d, n2, B, s.r3.m[0], w.rs_acc.p);
+  VIA_LAUNCHED();
+  from_eval(s.r3, w.rs_acc.p, n2, B * 2, st);
+  k_ring_switch_finish_batch<<<blocks(B * n2), 256, 0, st>>>(w.rs_acc.p, w.rs_bproj.p, n2, B, s.r3.m[0], s.r4.m[0],
+                                                             (double)p.q3, d_mask, d_body);
+  VIA_LAUNCHED();
+}
+
 // Runs the pipeline for nq queries (d_query: nq queries back to back; d_mask,
 // d_body: [nq][n2]). When stop_stage > 0 (nq == 1 only), copies that stage's
 // output in coefficient form to `dump` and returns early. Stages: 1 cascade
@@ -887,21 +909,8 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
     VIA_LAUNCHED();
   }
   if (stop_stage == 7) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
-
-  // ---- Step 7: RespComp (resp_comp.rs:46-76).
-  mod_switch(s.r2, w.cr_ct.p, s.r3n1, w.rs_ct3.p, B * 2, n1, st);
-  const int d = n1 / n2;
-  k_ring_switch_proj_batch<<<blocks(B * (d + 1) * n2), 256, 0, st>>>(w.rs_ct3.p, n1, n2, B, s.r3.m[0], w.rs_mproj.p,
-                                                                      w.rs_bproj.p);
-  VIA_LAUNCHED();
-  gadget_product(s.r3, w.g_rsk, w.rs_mproj.p, n2, 1, 1, B * d, keys_cyclic(s.rsk_eval.p, d), w.rs_gp.p,
-                 w.rs_digits.p, st);
-  k_ring_switch_sum_batch<<<blocks(B * 2 * n2), 256, 0, st>>>(w.rs_gp.p, d, n2, B, s.r3.m[0], w.rs_acc.p);
-  VIA_LAUNCHED();
-  from_eval(s.r3, w.rs_acc.p, n2, B * 2, st);
-  k_ring_switch_finish_batch<<<blocks(B * n2), 256, 0, st>>>(w.rs_acc.p, w.rs_bproj.p, n2, B, s.r3.m[0], s.r4.m[0],
-                                                             (double)p.q3, d_mask, d_body);
-  VIA_LAUNCHED();
+  if (stop_stage == STOP_AFTER_CROT) return;
+  resp_comp(s, w.cr_ct.p, B, d_mask, d_body, st);
 }
 
 void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st) {
@@ -944,6 +953,189 @@ void answer_graph(Server& s, int nq, cudaStream_t st) {
   }
   VIA_CUDA(cudaGraphLaunch(exec, st));
   __atomic_add_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);
+}
+
+
+// ===========================================================================
+// VIA-B: repack of T CRot outputs into one RLWE (crates/via-primitives/src/
+// conversion/repack.rs, crates/via-server/src/batch.rs:72-163).
+//
+// A level's list of MLWEs is stored as masks [count][rank][deg] and bodies
+// [count][deg] at q2, coefficient form. Extr_{n_rec} turns each CRot output into
+// an (n1/n_rec, n_rec)-MLWE; input t goes to position bitrev(t) (the reference
+// swaps the T inputs into bit-reversed order) and positions >= T are zero
+// MLWEs. Each level pairs entries (2p, 2p+1): embed_d interleaves the pair
+// (slots 0 and 1), every embedded mask is key-switched with the level's
+// q2-switched cascade keys, and conv_step's slot reduction gives
+// masks_out[j] = -(P[j].mask + P[j+R/2].mask), body = embed_d(bodies) - sum P.body.
+// Pairs of two zero MLWEs give zero MLWEs (zero digits), so only the leading
+// nonzero entries are processed.
+// ===========================================================================
+
+// masks/bodies of the level-0 list from the CRot outputs ct [T][2][n1].
+__global__ void k_repack_extr(const u64* __restrict__ ct, int T, int lt, int n1, int g, DevMod m, u64* __restrict__ masks,
+                              u64* __restrict__ bodies) {
+  const int D = n1 / g;
+  const long total = (long)T * (D + 1) * g;
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= total) return;
+  const int i = (int)(gid % g);
+  const int k = (int)((gid / g) % (D + 1));
+  const int t = (int)(gid / ((long)g * (D + 1)));
+  int pos = 0;
+  for (int b = 0; b < lt; ++b) pos |= ((t >> b) & 1) << (lt - 1 - b);
+  const u64* mask = ct + (long)t * 2 * n1;
+  const u64* body = mask + n1;
+  if (k == D) {
+    bodies[(long)pos * g + i] = body[(long)D * i];
+    return;
+  }
+  u64 v;
+  if (k == 0) {
+    v = mask[(long)D * i];
+  } else {
+    // (X * pi_{D-k}(A))[i]: pi[i-1], and -pi[g-1] at i = 0.
+    const int slot = D - k;
+    v = i == 0 ? negmod(mask[(long)D * (g - 1) + slot], m.q) : mask[(long)D * (i - 1) + slot];
+  }
+  masks[((long)pos * D + k) * g + i] = v;
+}
+
+// embed_d (d = 2) of `pairs` pairs: emb_masks [pair][rank][2 n_in], emb_body [pair][2 n_in].
+__global__ void k_repack_embed(const u64* __restrict__ masks, const u64* __restrict__ bodies, long pairs, int rank,
+                               int n_in, u64* __restrict__ emb_masks, u64* __restrict__ emb_body) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= pairs * (rank + 1) * n_in) return;
+  const int i = (int)(gid % n_in);
+  const int k = (int)((gid / n_in) % (rank + 1));
+  const long pr = gid / ((long)n_in * (rank + 1));
+  const int n_out = 2 * n_in;
+  if (k == rank) {
+    emb_body[pr * n_out + 2 * i] = bodies[(2 * pr) * n_in + i];
+    emb_body[pr * n_out + 2 * i + 1] = bodies[(2 * pr + 1) * n_in + i];
+    return;
+  }
+  u64* o = emb_masks + (pr * rank + k) * n_out;
+  o[2 * i] = masks[((2 * pr) * rank + k) * n_in + i];
+  o[2 * i + 1] = masks[((2 * pr + 1) * rank + k) * n_in + i];
+}
+
+__global__ void k_sub_polys(const u64* __restrict__ a, const u64* __restrict__ b, long count, DevMod m,
+                            u64* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count) return;
+  out[gid] = submod(a[gid], b[gid], m.q);
+}
+
+// The repack keys: for every output degree nout = 2 n_rec .. n1 the cascade step
+// of that degree (rank_in = 2 n1 / nout RLevs of L_CK samples), switched from q1
+// to q2 sample by sample (mod_switch_rlev, repack.rs:684-739) and transformed at
+// q2. Must run before the cascade key itself is transformed.
+void derive_repack_keys(Server& s) {
+  const via_params& p = s.prm;
+  if (via_b_batch(p) < 2 || !s.cascade_eval.p) return;
+  const int n1 = p.n1, L = p.l_ck, nl = s.r1.nl;
+  const u64 step_len = (u64)2 * n1 * L * 2 * nl;
+  size_t total = 0;
+  s.repack_off.clear();
+  for (int nout = 2 * (int)p.n_rec; nout <= n1; nout <<= 1) {
+    s.repack_off.push_back(total);
+    total += (size_t)(2 * n1 / nout) * L * 2 * nout;
+  }
+  s.repack_eval.alloc(total);
+  int level = 0;
+  for (int nout = 2 * (int)p.n_rec; nout <= n1; nout <<= 1, ++level) {
+    const int k = ilog2(nout);  // cascade step k has output degree 2^k
+    const long polys = (long)(2 * n1 / nout) * L * 2;
+    u64* dst = s.repack_eval.p + s.repack_off[level];
+    mod_switch(s.r1, s.cascade_eval.p + (k - 1) * step_len, s.r2, dst, polys, nout, s.stream);
+    to_eval(s.r2, dst, nout, polys, s.stream);
+  }
+}
+
+struct RepackWs {
+  int T = 0;
+  DevBuf la_m, la_b, lb_m, lb_b, emb_m, emb_b, digits, P, bsum, rlwe;
+  Gadget g;
+};
+
+// Called with the server's mutex held.
+static RepackWs& repack_ws(Server& s) {
+  Workspace& w = *s.ws;
+  if (!w.repack) {
+    const via_params& p = s.prm;
+    auto r = std::make_unique<RepackWs>();
+    const long T = via_b_batch(p), n1 = p.n1, L = p.l_ck;
+    const long pairs = std::max(1L, T / 2);
+    r->T = (int)T;
+    // Level lists hold at most T (+1 zero partner) entries of n1 + deg residues.
+    r->la_m.alloc((T + 2) * n1);
+    r->la_b.alloc((T + 2) * n1);
+    r->lb_m.alloc((T + 2) * n1);
+    r->lb_b.alloc((T + 2) * n1);
+    r->emb_m.alloc(pairs * 2 * n1);
+    r->emb_b.alloc(pairs * n1);
+    r->digits.alloc(pairs * 2 * n1 * L);
+    r->P.alloc(pairs * 4 * n1);
+    r->bsum.alloc(pairs * n1);
+    r->rlwe.alloc(2 * n1);
+    r->g = make_gadget(p.ck_base, (int)p.l_ck, s.r2.Q());
+    w.repack = std::move(r);
+  }
+  return *w.repack;
+}
+
+static void repack(Server& s, const u64* crot, u64* out_rlwe, cudaStream_t st) {
+  const via_params& p = s.prm;
+  RepackWs& r = repack_ws(s);
+  const int n1 = p.n1, g = (int)p.n_rec, T = r.T, D = n1 / g;
+  int lt = 0;
+  while ((1 << lt) < T) ++lt;
+  u64 *cm = r.la_m.p, *cb = r.la_b.p, *nm = r.lb_m.p, *nb = r.lb_b.p;
+  {
+    const long total = (long)T * (D + 1) * g;
+    k_repack_extr<<<blocks(total), 256, 0, st>>>(crot, T, lt, n1, g, s.r2.m[0], cm, cb);
+    VIA_LAUNCHED();
+  }
+  long active = T;  // leading nonzero entries of the current list
+  int rank = D, level = 0;
+  for (int n_in = g; n_in < n1; n_in <<= 1, rank >>= 1, ++level) {
+    const int n_out = 2 * n_in;
+    if (active & 1) {  // the last pair's partner is a zero MLWE
+      VIA_CUDA(cudaMemsetAsync(cm + active * rank * n_in, 0, (size_t)rank * n_in * 8, st));
+      VIA_CUDA(cudaMemsetAsync(cb + active * n_in, 0, (size_t)n_in * 8, st));
+    }
+    const long pairs = (active + 1) / 2;
+    k_repack_embed<<<blocks(pairs * (rank + 1) * n_in), 256, 0, st>>>(cm, cb, pairs, rank, n_in, r.emb_m.p, r.emb_b.p);
+    VIA_LAUNCHED();
+    gadget_product(s.r2, r.g, r.emb_m.p, n_out, 1, 1, pairs * rank,
+                   keys_cyclic(s.repack_eval.p + s.repack_off[level], rank), r.P.p, r.digits.p, st);
+    const long items = pairs * (rank / 2 + 1) * n_out;
+    k_cascade_reduce<<<blocks(items), 256, 0, st>>>(r.P.p, rank, n_out, 1, pairs, s.r2, nm, r.bsum.p);
+    VIA_LAUNCHED();
+    from_eval(s.r2, nm, n_out, pairs * (rank / 2), st);
+    from_eval(s.r2, r.bsum.p, n_out, pairs, st);
+    k_sub_polys<<<blocks(pairs * n_out), 256, 0, st>>>(r.emb_b.p, r.bsum.p, pairs * n_out, s.r2.m[0], nb);
+    VIA_LAUNCHED();
+    std::swap(cm, nm);
+    std::swap(cb, nb);
+    active = pairs;
+  }
+  // The rank-1 MLWE of degree n1 is the RLWE (mask, body).
+  VIA_CUDA(cudaMemcpyAsync(out_rlwe, cm, (size_t)n1 * 8, cudaMemcpyDeviceToDevice, st));
+  VIA_CUDA(cudaMemcpyAsync(out_rlwe + n1, cb, (size_t)n1 * 8, cudaMemcpyDeviceToDevice, st));
+}
+
+// answer_batch (srv/batch.rs:72-163): the prefix through CRot for the T queries
+// (sharing one database scan), the repack, and RespComp once.
+void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st) {
+  const int T = via_b_batch(s.prm);
+  if (T < 2) throw CudaError(100, "answer_batch: the server was set up for VIA-C (n_rec = n2)");
+  if (!s.repack_eval.p) throw CudaError(100, "answer_batch: no repack keys");
+  answer_device_stages(s, d_queries, T, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
+  RepackWs& r = repack_ws(s);
+  repack(s, s.ws->cr_ct.p, r.rlwe.p, st);
+  resp_comp(s, r.rlwe.p, 1, d_mask, d_body, st);
 }
 
 }  // namespace via

@@ -283,6 +283,7 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     VIA_CUDA(cudaMemcpyAsync(s.cascade_eval.p, keys->cascade_key, s.cascade_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
     VIA_CUDA(cudaMemcpyAsync(s.conv_eval.p, keys->conv_key, s.conv_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
     VIA_CUDA(cudaMemcpyAsync(s.rsk_eval.p, keys->rsk, s.rsk_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+    derive_repack_keys(s);  // VIA-B: from the coefficient-form cascade key, before it is transformed
     transform_keys(s);
   }
   workspace_create(s, 1);
@@ -489,6 +490,51 @@ via_status via_server_answer_many(via_server* s, const uint64_t* queries, uint64
                              s->stream));
     VIA_CUDA(cudaMemcpyAsync(out_bodies, workspace_answer_body(*s), n_queries * p.n2 * 8, cudaMemcpyDeviceToHost,
                              s->stream));
+    VIA_CUDA(cudaStreamSynchronize(s->stream));
+    check_device_flags(*s, s->stream);
+  });
+}
+
+static void check_batch(via_server* s, uint64_t n_queries, uint64_t n_lwe) {
+  const via_params& p = s->prm;
+  const u64 T = (u64)via_b_batch(p);
+  if (T < 2) throw ApiError(VIA_ERR_DIM_MISMATCH, "answer_batch: the server was set up for VIA-C (n_rec = n2)");
+  if (n_queries != T)
+    throw ApiError(VIA_ERR_DIM_MISMATCH, "answer_batch: batch.len() must equal T = n2 / n_rec = " + std::to_string(T));
+  if (n_lwe != query_lwes(p))
+    throw ApiError(VIA_ERR_QUERY_LENGTH_MISMATCH, "query length mismatch: expected " + std::to_string(query_lwes(p)) +
+                                                      " ciphertexts, got " + std::to_string(n_lwe));
+  if (!s->cascade_eval.p) throw ApiError(VIA_ERR_SETUP_NOT_COMPLETE, "server has no public keys");
+}
+
+via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                       uint64_t* out_mask, uint64_t* out_body, void* stream) {
+  return guarded([&] {
+    if (!s || !queries || !out_mask || !out_body) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    check_batch(s, n_queries, n_lwe);
+    const via_params& p = s->prm;
+    cudaStream_t st = (cudaStream_t)stream;
+    std::lock_guard<std::mutex> g(s->mu);
+    ensure_batch(s, n_queries);
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
+                             cudaMemcpyDeviceToDevice, st));
+    answer_batch_device(*s, workspace_query(*s), out_mask, out_body, st);
+  });
+}
+
+via_status via_server_answer_batch(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
+                                   uint64_t* out_mask, uint64_t* out_body) {
+  return guarded([&] {
+    if (!s || !queries || !out_mask || !out_body) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    check_batch(s, n_queries, n_lwe);
+    const via_params& p = s->prm;
+    std::lock_guard<std::mutex> g(s->mu);
+    ensure_batch(s, n_queries);
+    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
+                             cudaMemcpyHostToDevice, s->stream));
+    answer_batch_device(*s, workspace_query(*s), workspace_answer_mask(*s), workspace_answer_body(*s), s->stream);
+    VIA_CUDA(cudaMemcpyAsync(out_mask, workspace_answer_mask(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
+    VIA_CUDA(cudaMemcpyAsync(out_body, workspace_answer_body(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));
     check_device_flags(*s, s->stream);
   });

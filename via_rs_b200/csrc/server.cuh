@@ -60,6 +60,10 @@ struct Server {
   DevBuf cascade_eval;  // include/via_gpu.h cascade layout, each segment transformed
   DevBuf conv_eval;     // L_CK samples at (q1, n1)
   DevBuf rsk_eval;      // d RLevs at (q3, n2)
+  // VIA-B repack keys (n_rec < n2): the cascade steps of output degree 2 n_rec .. n1,
+  // every sample switched q1 -> q2 and in eval form at q2; level l starts at repack_off[l].
+  DevBuf repack_eval;
+  std::vector<size_t> repack_off;
   std::unique_ptr<Workspace, WorkspaceDeleter> ws;
   std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
   bool tensor_fd() const { return fd.planes != nullptr; }
@@ -76,6 +80,11 @@ u64 rsk_len(const via_params& p);
 int ilog2(u64 v);
 
 // Pipeline entry points (pipeline.cu).
+constexpr int STOP_AFTER_CROT = -1;  // answer_device_stages: leave the CRot outputs in the workspace
+// VIA-B batch size T = n2 / n_rec (the record-fit boundary); 1 for VIA-C servers.
+inline int via_b_batch(const via_params& p) { return (int)(p.n2 / p.n_rec); }
+void derive_repack_keys(Server& s);
+void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st);
 void workspace_create(Server& s, int bmax);
 int workspace_batch(Server& s);
 void workspace_destroy(Server& s);

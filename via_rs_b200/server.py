@@ -159,6 +159,23 @@ class Server:
         check(_lib.lib().via_first_dim_dev(self._h, ctypes.c_void_p(switched_ptr), ctypes.c_void_p(out_ptr),
                                            ctypes.c_void_p(stream)))
 
+    def answer_batch(self, queries):
+        """Server::answer_batch (VIA-B): T = n2 / n_rec queries, one answer (mask, body).
+
+        queries: (T, n_lwe * lwe_len). Raises DimMismatch when the count is not T and
+        QueryLengthMismatch when a query does not hold n_lwe LWEs.
+        """
+        prm = self.prm
+        q = np.ascontiguousarray(queries, dtype=np.uint64)
+        if q.ndim != 2 or q.shape[1] % prm.lwe_len:
+            raise BufferTooShort("queries must be (T, n_lwe * lwe_len)")
+        mask = np.zeros(prm.n2, dtype=np.uint64)
+        body = np.zeros(prm.n2, dtype=np.uint64)
+        check(_lib.lib().via_server_answer_batch(self._h, q.ctypes.data_as(ctypes.c_void_p), q.shape[0],
+                                                 q.shape[1] // prm.lwe_len, mask.ctypes.data_as(ctypes.c_void_p),
+                                                 body.ctypes.data_as(ctypes.c_void_p)))
+        return mask, body
+
     def scan_dev(self, sel_eval_ptr: int, out_eval_ptr: int, stream: int = 0) -> None:
         """The FirstDim scan alone on eval-form device buffers (one query)."""
         check(_lib.lib().via_first_dim_scan_dev(self._h, ctypes.c_void_p(sel_eval_ptr), ctypes.c_void_p(out_eval_ptr),
