@@ -214,6 +214,55 @@ via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, u
                                        uint64_t* out_mask, uint64_t* out_body, void* stream);
 
 /*
+ * Serving: a continuous-batching answer service over one server handle (the
+ * request loop the reference leaves to its caller). Requests are queued on
+ * the host; a worker thread keeps `lanes` batches in flight, each on its own
+ * stream and workspace, and whenever a lane frees up it takes every pending
+ * request up to the lane's capacity (one database scan per batch). The
+ * capacity is the largest batch whose workspace fits hbm_budget / lanes, capped
+ * by max_batch; requests beyond it wait for a free lane. A VIA-C server serves
+ * single queries; a VIA-B server (n_rec < n2) serves groups of T = n2 / n_rec
+ * queries, one answer per group. Results do not depend on how requests are
+ * batched. Every wait is bounded; no host thread blocks inside the driver.
+ */
+typedef struct via_service via_service;
+
+typedef struct {
+  uint32_t lanes;       /* batches in flight; 0 -> 2 */
+  uint32_t max_batch;   /* requests per batch; 0 -> 64 */
+  uint64_t hbm_budget;  /* device bytes for all lanes' workspaces; 0 -> max_batch decides */
+  uint32_t max_pending; /* queued requests before submit returns VIA_ERR_BUSY; 0 -> 2^20 */
+  uint32_t reserved;
+} via_service_config;
+
+typedef struct {
+  uint64_t submitted, completed, failed, batches, units;
+  uint32_t lanes, batch_cap;
+  uint32_t max_in_flight; /* most batches seen on the GPU at once */
+  uint32_t reserved;
+  double p50_ms, p99_ms;  /* submit-to-completion latency of completed requests */
+  double mean_batch;      /* requests per launched batch */
+  double answers_per_s;   /* completed requests / (last completion - first submit) */
+} via_service_stats;
+
+via_status via_service_create(via_server* s, const via_service_config* cfg, via_service** out);
+/* Device bytes of one lane's workspace for batches of up to max_queries queries
+ * (for sizing hbm_budget); 0 on a null handle. */
+uint64_t via_server_workspace_bytes(via_server* s, uint64_t max_queries);
+/* Queues one request: a query of n_lwe LWEs (VIA-C) or T such queries back to
+ * back (VIA-B); the buffer is copied. Returns a ticket. */
+via_status via_service_submit(via_service* v, const uint64_t* query, uint64_t n_lwe, uint64_t* ticket);
+/* Non-blocking: *done = 1 and the answer (n2 + n2 residues) once finished; the
+ * ticket is then released. */
+via_status via_service_poll(via_service* v, uint64_t ticket, uint64_t* out_mask, uint64_t* out_body, int* done);
+/* Waits up to timeout_ms (VIA_ERR_TIMEOUT after that, the ticket stays valid). */
+via_status via_service_wait(via_service* v, uint64_t ticket, uint64_t* out_mask, uint64_t* out_body,
+                            uint32_t timeout_ms);
+via_status via_service_stats_get(via_service* v, via_service_stats* out);
+/* Finishes the batches on the GPU, drops queued requests, frees the lanes. */
+void via_service_destroy(via_service* v);
+
+/*
  * The FirstDim scan of via_first_dim_scan_dev for callers that cannot allocate
  * device memory: code that runs where cudaMalloc is not allowed or not wanted
  * (inside a region being captured into a CUDA graph, a host whose allocator is

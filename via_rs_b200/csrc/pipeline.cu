@@ -425,8 +425,10 @@ struct Workspace {
   std::vector<std::pair<int, cudaGraphExec_t>> graphs;  // one per batch size
   std::vector<std::pair<int, unsigned long long>> graph_kernels;
   std::unique_ptr<struct RepackWs> repack;  // VIA-B buffers, made on the first batch answer
+  cudaStream_t capture = nullptr;           // stream the answer graphs are captured on
   ~Workspace() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
+    if (capture) cudaStreamDestroy(capture);
   }
 };
 
@@ -445,62 +447,89 @@ void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, ui
                          (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], st);
 }
 
-void workspace_create(Server& s, int bmax) {
+static bool cmux_fused_ok(const DevRing& R, const Gadget& g);
+
+// Allocates a workspace for batches of up to bmax queries, or (count_only)
+// returns the bytes it would take.
+static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only) {
   const via_params& p = s.prm;
-  auto w = std::make_unique<Workspace>();
+  size_t bytes = 0;
+  auto A = [&](DevBuf& b, long count) {
+    bytes += (size_t)std::max(0L, count) * 8;
+    if (!count_only) b.alloc((size_t)std::max(0L, count));
+  };
   const long n1 = p.n1, n2 = p.n2, nl = s.r1.nl, L = p.l_query, Lck = p.l_ck, I = p.num_rows, J = p.num_cols;
   const long B = std::max(1, bmax);
   w->bmax = (int)B;
   w->nlwe = (long)query_lwes(p);
   w->nbits = w->nlwe / L;
   const long nlwe = w->nlwe * B;  // LWEs of a full batch
-  w->c_masks_a.alloc(nlwe * n1 * nl);
-  w->c_masks_b.alloc(nlwe * n1 * nl);
-  w->c_body_a.alloc(nlwe * n1 * nl);
-  w->c_body_b.alloc(nlwe * n1 * nl);
-  w->c_digits.alloc(nlwe * 2 * n1 * Lck * nl);
-  w->c_P.alloc(nlwe * 2 * n1 * 2 * nl);
-  w->c_bsum.alloc(nlwe * n1 * nl);
-  w->c_rlwe.alloc(nlwe * 2 * n1 * nl);
-  w->g_digits.alloc(nlwe * Lck * nl * n1);
-  w->g_gp.alloc(nlwe * 2 * nl * n1);
-  w->rgsw_q1.alloc(B * w->nbits * 2 * L * 2 * nl * n1);
-  w->rgsw_q2.alloc(B * w->nbits * 2 * L * 2 * n1);
-  w->dm_a.alloc(B * I * 2 * nl * n1);
-  w->dm_b.alloc(B * I * 2 * nl * n1);
-  w->dm_digits.alloc(B * std::max(1L, I / 2) * 2 * L * nl * n1);
-  w->dm_ext.alloc(B * std::max(1L, I / 2) * 2 * nl * n1);
-  w->sel.alloc(B * I * 2 * n1);
+  A(w->c_masks_a, nlwe * n1 * nl);
+  A(w->c_masks_b, nlwe * n1 * nl);
+  A(w->c_body_a, nlwe * n1 * nl);
+  A(w->c_body_b, nlwe * n1 * nl);
+  // NTT rings transform the cascade digits at the input degree (half of the
+  // embedded degree); the other rings use the embedded digits and the P buffer.
+  A(w->c_digits, nlwe * (s.r1.ntt ? 1 : 2) * n1 * Lck * nl);
+  A(w->c_P, s.r1.ntt ? 0 : nlwe * 2 * n1 * 2 * nl);
+  A(w->c_bsum, nlwe * n1 * nl);
+  A(w->c_rlwe, nlwe * 2 * n1 * nl);
+  A(w->g_digits, nlwe * Lck * nl * n1);
+  A(w->g_gp, nlwe * 2 * nl * n1);
+  A(w->rgsw_q1, B * w->nbits * 2 * L * 2 * nl * n1);
+  A(w->rgsw_q2, B * w->nbits * 2 * L * 2 * n1);
+  A(w->dm_a, B * I * 2 * nl * n1);
+  A(w->dm_b, B * I * 2 * nl * n1);
+  A(w->dm_digits, B * std::max(1L, I / 2) * 2 * L * nl * n1);
+  A(w->dm_ext, B * std::max(1L, I / 2) * 2 * nl * n1);
+  A(w->sel, B * I * 2 * n1);
   if (s.tensor_fd()) {
     size_t bytes = 0;  // the split selection grows with the batch; size it for every batch up to B
     for (int nq = 1; nq <= B; ++nq) bytes = std::max(bytes, fd_sel_bytes(s.fd, nq));
-    w->sel_bytes.alloc((bytes + 7) / 8);
+    A(w->sel_bytes, (bytes + 7) / 8);
   }
-  w->fd_out.alloc(B * J * 2 * n1);
-  w->cm_diff.alloc(B * std::max(1L, J / 2) * 2 * n1);
-  w->cm_digits.alloc(B * std::max(1L, J / 2) * 2 * L * n1);
-  w->cm_ext.alloc(B * std::max(1L, J / 2) * 2 * n1);
-  w->cm_b.alloc(B * std::max(1L, J / 2) * 2 * n1);
-  w->cr_ct.alloc(B * 2 * n1);
-  w->cr_diff.alloc(B * 2 * n1);
-  w->cr_digits.alloc(B * 2 * L * n1);
-  w->cr_ext.alloc(B * 2 * n1);
-  w->rs_ct3.alloc(B * 2 * n1);
+  A(w->fd_out, B * J * 2 * n1);
+  const bool fused = cmux_fused_ok(s.r2, make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q()));
+  A(w->cm_diff, fused ? 0 : B * std::max(1L, J / 2) * 2 * n1);
+  A(w->cm_digits, fused ? 0 : B * std::max(1L, J / 2) * 2 * L * n1);
+  A(w->cm_ext, fused ? 0 : B * std::max(1L, J / 2) * 2 * n1);
+  A(w->cm_b, B * std::max(1L, J / 2) * 2 * n1);
+  A(w->cr_ct, B * 2 * n1);
+  A(w->cr_diff, B * 2 * n1);
+  A(w->cr_digits, B * 2 * L * n1);
+  A(w->cr_ext, B * 2 * n1);
+  A(w->rs_ct3, B * 2 * n1);
   long d = n1 / n2;
-  w->rs_mproj.alloc(B * d * n2);
-  w->rs_bproj.alloc(B * n2);
-  w->rs_digits.alloc(B * d * p.l_rsk * n2);
-  w->rs_gp.alloc(B * d * 2 * n2);
-  w->rs_acc.alloc(B * 2 * n2);
-  w->q_in.alloc(nlwe * lwe_len(p));
-  w->a_mask.alloc(B * n2);
-  w->a_body.alloc(B * n2);
+  A(w->rs_mproj, B * d * n2);
+  A(w->rs_bproj, B * n2);
+  A(w->rs_digits, B * d * p.l_rsk * n2);
+  A(w->rs_gp, B * d * 2 * n2);
+  A(w->rs_acc, B * 2 * n2);
+  A(w->q_in, nlwe * lwe_len(p));
+  A(w->a_mask, B * n2);
+  A(w->a_body, B * n2);
+  if (count_only) return bytes;
   w->g_ck = make_gadget(p.ck_base, (int)p.l_ck, s.r1.Q());
   w->g_dmux = make_gadget(p.b_dmux, (int)p.l_query, s.r1.Q());
   w->g_cmux = make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q());
   w->g_rsk = make_gadget(p.b_rsk, (int)p.l_rsk, s.r3.Q());
-  s.ws.reset(w.release());
+  return bytes;
 }
+
+std::unique_ptr<Workspace, WorkspaceDeleter> workspace_make(Server& s, int bmax) {
+  std::unique_ptr<Workspace, WorkspaceDeleter> w(new Workspace());
+  workspace_build(s, bmax, w.get(), false);
+  VIA_CUDA(cudaStreamCreateWithFlags(&w->capture, cudaStreamNonBlocking));
+  return w;
+}
+
+size_t workspace_bytes(Server& s, int bmax) {
+  Workspace scratch;
+  return workspace_build(s, bmax, &scratch, true);
+}
+
+void workspace_create(Server& s, int bmax) { s.ws = workspace_make(s, bmax); }
+
 
 int workspace_batch(Server& s) { return s.ws ? s.ws->bmax : 0; }
 
@@ -547,8 +576,7 @@ static void mod_switch(const DevRing& S, const u64* in, const DevRing& D, u64* o
 }
 
 // Step 1: QueryDecomp for nq queries -> rgsw_q1 [q][nbits][2L][2][nl][n1] (coefficient form).
-static void query_decomp(Server& s, const u64* d_query, int nq, cudaStream_t st) {
-  Workspace& w = *s.ws;
+static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cudaStream_t st) {
   const via_params& p = s.prm;
   const DevRing& R = s.r1;
   const int n1 = p.n1, nl = R.nl, L = p.l_ck;
@@ -791,8 +819,8 @@ __global__ void k_ring_switch_finish_batch(const u64* acc, const u64* body_proj,
 
 // Step 7, RespComp (resp_comp.rs:46-76), of B RLWEs at (q2, n1) in coefficient
 // form: q2 -> q3, ring switch n1 -> n2 with the RSK, body q3 -> q4.
-static void resp_comp(Server& s, const u64* ct_q2, long B, u64* d_mask, u64* d_body, cudaStream_t st) {
-  Workspace& w = *s.ws;
+static void resp_comp(Server& s, Workspace& w, const u64* ct_q2, long B, u64* d_mask, u64* d_body,
+                      cudaStream_t st) {
   const via_params& p = s.prm;
   const int n1 = p.n1, n2 = p.n2;
   mod_switch(s.r2, ct_q2, s.r3n1, w.rs_ct3.p, B * 2, n1, st);
@@ -815,9 +843,8 @@ static void resp_comp(Server& s, const u64* ct_q2, long B, u64* d_mask, u64* d_b
 // output in coefficient form to `dump` and returns early. Stages: 1 cascade
 // RLWEs, 2 query RGSWs at q1, 3 DMux outputs, 4 mod-switched rows at q2,
 // 5 FirstDim columns, 6 CMux output, 7 CRot output.
-void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u64* d_body, cudaStream_t st,
-                          int stop_stage, u64* dump) {
-  Workspace& w = *s.ws;
+void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u64* d_mask, u64* d_body,
+                          cudaStream_t st, int stop_stage, u64* dump) {
   const via_params& p = s.prm;
   const int n1 = p.n1, n2 = p.n2, L = p.l_query, nl = s.r1.nl;
   const long I = p.num_rows, J = p.num_cols, B = nq;
@@ -829,7 +856,7 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
     VIA_CUDA(cudaMemcpyAsync(dump, src, count * 8, cudaMemcpyDeviceToDevice, st));
   };
   // ---- Step 1: QueryDecomp.
-  query_decomp(s, d_query, nq, st);
+  query_decomp(s, w, d_query, nq, st);
   if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
   if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
 
@@ -866,7 +893,7 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
   // ---- Step 4: FirstDim (answer.rs:204-205), one pass over the database for
   // the whole batch; the columns stay in the eval domain.
   to_eval(s.r2, w.sel.p, n1, B * 2 * I, st);
-  first_dim_queries(s, w.sel.p, w.fd_out.p, nq, workspace_sel_bytes(s), st);
+  first_dim_queries(s, w.sel.p, w.fd_out.p, nq, reinterpret_cast<uint8_t*>(w.sel_bytes.p), st);
   if (stop_stage == 5) {
     copy_out(w.fd_out.p, (size_t)J * 2 * n1);
     from_eval(s.r2, dump, n1, 2 * J, st);
@@ -910,21 +937,28 @@ void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u6
   }
   if (stop_stage == 7) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
   if (stop_stage == STOP_AFTER_CROT) return;
-  resp_comp(s, w.cr_ct.p, B, d_mask, d_body, st);
+  resp_comp(s, w, w.cr_ct.p, B, d_mask, d_body, st);
+}
+
+void answer_device_stages(Server& s, const u64* d_query, int nq, u64* d_mask, u64* d_body, cudaStream_t st,
+                          int stop_stage, u64* dump) {
+  answer_device_stages(s, *s.ws, d_query, nq, d_mask, d_body, st, stop_stage, dump);
 }
 
 void answer_device(Server& s, const u64* d_query, u64* d_mask, u64* d_body, cudaStream_t st) {
   answer_device_stages(s, d_query, 1, d_mask, d_body, st, 0, nullptr);
 }
 
+u64* ws_query(Workspace& w) { return w.q_in.p; }
+u64* ws_answer_mask(Workspace& w) { return w.a_mask.p; }
+u64* ws_answer_body(Workspace& w) { return w.a_body.p; }
 u64* workspace_query(Server& s) { return s.ws->q_in.p; }
 u64* workspace_answer_mask(Server& s) { return s.ws->a_mask.p; }
 u64* workspace_answer_body(Server& s) { return s.ws->a_body.p; }
 
 // The whole answer for nq queries (~220 kernels) on the workspace buffers,
 // captured once per batch size into a CUDA graph and replayed.
-void answer_graph(Server& s, int nq, cudaStream_t st) {
-  Workspace& w = *s.ws;
+void answer_graph(Server& s, Workspace& w, int nq, cudaStream_t st) {
   cudaGraphExec_t exec = nullptr;
   unsigned long long kernels = 0;
   for (size_t i = 0; i < w.graphs.size(); ++i)
@@ -935,14 +969,14 @@ void answer_graph(Server& s, int nq, cudaStream_t st) {
   if (!exec) {
     cudaGraph_t g;
     unsigned long long before = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED);
-    VIA_CUDA(cudaStreamBeginCapture(s.stream, cudaStreamCaptureModeThreadLocal));
+    VIA_CUDA(cudaStreamBeginCapture(w.capture, cudaStreamCaptureModeThreadLocal));
     try {
-      answer_device_stages(s, w.q_in.p, nq, w.a_mask.p, w.a_body.p, s.stream, 0, nullptr);
+      answer_device_stages(s, w, w.q_in.p, nq, w.a_mask.p, w.a_body.p, w.capture, 0, nullptr);
     } catch (...) {
-      cudaStreamEndCapture(s.stream, &g);
+      cudaStreamEndCapture(w.capture, &g);
       throw;
     }
-    VIA_CUDA(cudaStreamEndCapture(s.stream, &g));
+    VIA_CUDA(cudaStreamEndCapture(w.capture, &g));
     kernels = __atomic_load_n(&g_kernel_launches, __ATOMIC_RELAXED) - before;
     __atomic_sub_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);  // captured, not run
     cudaError_t e = cudaGraphInstantiate(&exec, g, 0);
@@ -954,6 +988,8 @@ void answer_graph(Server& s, int nq, cudaStream_t st) {
   VIA_CUDA(cudaGraphLaunch(exec, st));
   __atomic_add_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);
 }
+
+void answer_graph(Server& s, int nq, cudaStream_t st) { answer_graph(s, *s.ws, nq, st); }
 
 
 // ===========================================================================
@@ -1055,13 +1091,12 @@ void derive_repack_keys(Server& s) {
 
 struct RepackWs {
   int T = 0;
-  DevBuf la_m, la_b, lb_m, lb_b, emb_m, emb_b, digits, P, bsum, rlwe;
+  DevBuf la_m, la_b, lb_m, lb_b, emb_m, emb_b, digits, P, bsum, packed;
   Gadget g;
 };
 
-// Called with the server's mutex held.
-static RepackWs& repack_ws(Server& s) {
-  Workspace& w = *s.ws;
+// Called with the workspace owned by the caller.
+static RepackWs& repack_ws(Server& s, Workspace& w) {
   if (!w.repack) {
     const via_params& p = s.prm;
     auto r = std::make_unique<RepackWs>();
@@ -1078,16 +1113,15 @@ static RepackWs& repack_ws(Server& s) {
     r->digits.alloc(pairs * 2 * n1 * L);
     r->P.alloc(pairs * 4 * n1);
     r->bsum.alloc(pairs * n1);
-    r->rlwe.alloc(2 * n1);
     r->g = make_gadget(p.ck_base, (int)p.l_ck, s.r2.Q());
     w.repack = std::move(r);
   }
   return *w.repack;
 }
 
-static void repack(Server& s, const u64* crot, u64* out_rlwe, cudaStream_t st) {
+static void repack(Server& s, Workspace& w, const u64* crot, u64* out_rlwe, cudaStream_t st) {
   const via_params& p = s.prm;
-  RepackWs& r = repack_ws(s);
+  RepackWs& r = repack_ws(s, w);
   const int n1 = p.n1, g = (int)p.n_rec, T = r.T, D = n1 / g;
   int lt = 0;
   while ((1 << lt) < T) ++lt;
@@ -1128,14 +1162,24 @@ static void repack(Server& s, const u64* crot, u64* out_rlwe, cudaStream_t st) {
 
 // answer_batch (srv/batch.rs:72-163): the prefix through CRot for the T queries
 // (sharing one database scan), the repack, and RespComp once.
-void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st) {
+// `groups` VIA-B batches of T queries each (d_queries back to back); answer g
+// goes to d_mask/d_body + g * n2.
+void answer_batch_device(Server& s, Workspace& w, const u64* d_queries, int groups, u64* d_mask, u64* d_body,
+                         cudaStream_t st) {
   const int T = via_b_batch(s.prm);
+  const int n1 = s.prm.n1;
   if (T < 2) throw CudaError(100, "answer_batch: the server was set up for VIA-C (n_rec = n2)");
   if (!s.repack_eval.p) throw CudaError(100, "answer_batch: no repack keys");
-  answer_device_stages(s, d_queries, T, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
-  RepackWs& r = repack_ws(s);
-  repack(s, s.ws->cr_ct.p, r.rlwe.p, st);
-  resp_comp(s, r.rlwe.p, 1, d_mask, d_body, st);
+  answer_device_stages(s, w, d_queries, T * groups, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
+  RepackWs& r = repack_ws(s, w);
+  if (!r.packed.p || r.packed.n < (size_t)groups * 2 * n1) r.packed.alloc((size_t)groups * 2 * n1);
+  for (int g = 0; g < groups; ++g)
+    repack(s, w, w.cr_ct.p + (size_t)g * T * 2 * n1, r.packed.p + (size_t)g * 2 * n1, st);
+  resp_comp(s, w, r.packed.p, groups, d_mask, d_body, st);
+}
+
+void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st) {
+  answer_batch_device(s, *s.ws, d_queries, 1, d_mask, d_body, st);
 }
 
 }  // namespace via

@@ -26,6 +26,8 @@ static __device__ __align__(256) uint4 g_scan_scratch[STATIC_SCAN_SCRATCH / 16];
 static std::mutex g_scan_scratch_mu;
 static uint8_t* g_scan_scratch_addr[128] = {nullptr};
 
+void set_last_error(const std::string& m) { g_last_error = m; }
+
 template <class F>
 static via_status guarded(F&& f) {
   try {

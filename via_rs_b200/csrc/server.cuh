@@ -3,6 +3,7 @@
 #pragma once
 #include <memory>
 #include <mutex>
+#include <string>
 #include <vector>
 
 #include "../../include/via_gpu.h"
@@ -71,6 +72,7 @@ struct Server {
 };
 
 // Shared helpers.
+void set_last_error(const std::string& m);  // the message via_last_error() returns
 void validate_params(const via_params& p);
 u64 lwe_len(const via_params& p);
 u64 query_lwes(const via_params& p);
@@ -86,6 +88,14 @@ inline int via_b_batch(const via_params& p) { return (int)(p.n2 / p.n_rec); }
 void derive_repack_keys(Server& s);
 void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st);
 void workspace_create(Server& s, int bmax);
+std::unique_ptr<Workspace, WorkspaceDeleter> workspace_make(Server& s, int bmax);
+size_t workspace_bytes(Server& s, int bmax);  // device bytes of a workspace for bmax queries
+u64* ws_query(Workspace& w);
+u64* ws_answer_mask(Workspace& w);
+u64* ws_answer_body(Workspace& w);
+void answer_graph(Server& s, Workspace& w, int nq, cudaStream_t st);
+void answer_batch_device(Server& s, Workspace& w, const u64* d_queries, int groups, u64* d_mask, u64* d_body,
+                         cudaStream_t st);
 int workspace_batch(Server& s);
 void workspace_destroy(Server& s);
 uint8_t* workspace_sel_bytes(Server& s);
