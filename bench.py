@@ -57,6 +57,9 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true", help="skip the CPU oracle leg (for profiling)")
     ap.add_argument("--scan-launches", type=int, default=10)
     ap.add_argument("--batch", type=int, default=64, help="queries per shared-scan batch (0 = skip)")
+    ap.add_argument("--served", type=int, default=384,
+                    help="requests of the served leg (Poisson arrivals, continuous batching; 0 = skip)")
+    ap.add_argument("--via-b", type=int, default=1, help="run the VIA-B leg (T = 8, records of degree 64)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="set up, answer one batch of --batch queries and exit (a short target for ncu)")
     return ap.parse_args()
@@ -203,6 +206,79 @@ def config_dict(prm):
 # ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
+def served_leg(args, prm, server, query, rate):
+    """Seeded Poisson arrivals at `rate` requests/s into a 2-lane service; returns
+    throughput and the service's p50/p99 submit-to-answer latency."""
+    from via_rs_b200.service import Service
+
+    rng = np.random.default_rng(7)
+    gaps = rng.exponential(1.0 / rate, size=args.served)
+    svc = Service(server, lanes=2, max_batch=64, warm=True)  # graphs of every batch size captured up front
+    try:
+        for t in [svc.submit(query) for _ in range(4)]:
+            svc.wait(t)
+        svc.reset_stats()
+        tickets = []
+        t0 = time.perf_counter()
+        due = t0
+        for g in gaps:
+            due += g
+            while time.perf_counter() < due:
+                time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+            tickets.append(svc.submit(query))
+        for t in tickets:
+            svc.wait(t)
+        wall = time.perf_counter() - t0
+        st = svc.stats()
+    finally:
+        svc.close()
+    return {"requests": args.served, "offered_rate_hz": rate, "answers_s": st["answers_per_s"],
+            "wall_answers_s": args.served / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
+            "mean_batch": st["mean_batch"], "batches": st["batches"], "lanes": st["lanes"],
+            "max_in_flight": st["max_in_flight"], "arrivals": "seeded Poisson (numpy PCG64 seed 7)"}
+
+
+def via_b_leg(args, prm, rank):
+    """answer_batch with T = n2 / n3 = 8 queries per answer over the same number
+    of database cells (records of degree 64: 8x the records of the VIA-C leg)."""
+    import torch
+
+    from via_rs_b200.params import paper_preset
+    from via_rs_b200.server import VIA_RECORDS_NIBBLE, Server, check
+    from via_rs_b200 import _lib
+
+    pb = paper_preset(prm.num_rows, prm.num_cols, n_rec=64)
+    T = pb.n2 // pb.n_rec
+    records, keys, query = make_inputs(pb, seed=100 + rank)
+    srv = Server.setup(pb, keys, records, VIA_RECORDS_NIBBLE)
+    del records
+    L = _lib.lib()
+    qs = torch.from_numpy(np.tile(query, T).view(np.int64)).cuda()
+    dm = torch.empty(pb.n2, dtype=torch.int64, device="cuda")
+    db = torch.empty(pb.n2, dtype=torch.int64, device="cuda")
+    stream = torch.cuda.Stream()
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def one():
+        check(L.via_server_answer_batch_dev(srv._h, ctypes.c_void_p(qs.data_ptr()), T, pb.n_lwe,
+                                            ctypes.c_void_p(dm.data_ptr()), ctypes.c_void_p(db.data_ptr()), sptr))
+
+    for _ in range(2):
+        one()
+    torch.cuda.synchronize()
+    k = max(2, args.steps // 4)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(k):
+        one()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / k
+    srv.close()
+    return {"T": T, "record_degree": pb.n_rec, "ms_per_answer": ms, "answers_s": 1e3 / ms,
+            "records_s": T * 1e3 / ms, "db_raw_bytes": pb.capacity * pb.n_rec // 2}
+
+
 def gpu_arm(args, prm):
     import torch
 
@@ -332,6 +408,16 @@ def gpu_arm(args, prm):
                    "p99_ms": float(np.percentile(b_ms, 99)), "vs_plain": b_value / value}
         del d_qb, d_mb, d_bb
 
+    # ---- served: Poisson arrivals through the continuous-batching service.
+    served = None
+    if args.served > 0:
+        served = served_leg(args, prm, server, query, rate=0.85 * (batched["answers_s"] if batched else value))
+
+    # ---- VIA-B: T = 8 records of degree 64 per answer on a second (1 GiB) server.
+    via_b = None
+    if args.via_b and world == 1:
+        via_b = via_b_leg(args, prm, rank)
+
     # ---- roofline of the dominant kernel: the FirstDim scan alone, timed live.
     sel = torch.randint(0, prm.q2, (prm.num_rows * 2 * prm.n1,), dtype=torch.int64, device="cuda")
     out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
@@ -361,6 +447,8 @@ def gpu_arm(args, prm):
             "plain": {"answers_s": value, "db_gbs": value * db_bytes / 1e9, "db_raw_gbs": value * (1 << 30) / 1e9,
                       "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
             "batched": batched,
+            "served": served,
+            "via_b": via_b,
             "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols

@@ -232,7 +232,7 @@ typedef struct {
   uint32_t max_batch;   /* requests per batch; 0 -> 64 */
   uint64_t hbm_budget;  /* device bytes for all lanes' workspaces; 0 -> max_batch decides */
   uint32_t max_pending; /* queued requests before submit returns VIA_ERR_BUSY; 0 -> 2^20 */
-  uint32_t reserved;
+  uint32_t warm;        /* nonzero: capture every batch size's answer graph at creation */
 } via_service_config;
 
 typedef struct {
@@ -259,6 +259,8 @@ via_status via_service_poll(via_service* v, uint64_t ticket, uint64_t* out_mask,
 via_status via_service_wait(via_service* v, uint64_t ticket, uint64_t* out_mask, uint64_t* out_body,
                             uint32_t timeout_ms);
 via_status via_service_stats_get(via_service* v, via_service_stats* out);
+/* Zeroes the counters and latency record (requests in flight still complete). */
+via_status via_service_stats_reset(via_service* v);
 /* Finishes the batches on the GPU, drops queued requests, frees the lanes. */
 void via_service_destroy(via_service* v);
 

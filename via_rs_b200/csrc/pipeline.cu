@@ -958,6 +958,7 @@ u64* workspace_answer_body(Server& s) { return s.ws->a_body.p; }
 
 // The whole answer for nq queries (~220 kernels) on the workspace buffers,
 // captured once per batch size into a CUDA graph and replayed.
+// st == nullptr captures (if needed) without launching.
 void answer_graph(Server& s, Workspace& w, int nq, cudaStream_t st) {
   cudaGraphExec_t exec = nullptr;
   unsigned long long kernels = 0;
@@ -985,11 +986,12 @@ void answer_graph(Server& s, Workspace& w, int nq, cudaStream_t st) {
     w.graphs.push_back({nq, exec});
     w.graph_kernels.push_back({nq, kernels});
   }
+  if (!st) return;
   VIA_CUDA(cudaGraphLaunch(exec, st));
   __atomic_add_fetch(&g_kernel_launches, kernels, __ATOMIC_RELAXED);
 }
 
-void answer_graph(Server& s, int nq, cudaStream_t st) { answer_graph(s, *s.ws, nq, st); }
+void answer_graph(Server& s, int nq, cudaStream_t st) { answer_graph(s, *s.ws, nq, st ? st : s.stream); }
 
 
 // ===========================================================================

@@ -260,6 +260,8 @@ via_status via_service_create(via_server* s, const via_service_config* cfg, via_
       VIA_CUDA(cudaHostAlloc((void**)&L.h_body, (size_t)cap * p.n2 * 8, cudaHostAllocDefault));
       VIA_CUDA(cudaHostAlloc((void**)&L.h_err, sizeof(int), cudaHostAllocDefault));
       *L.h_err = 0;
+      if (c.warm && !v->via_b)  // capture the answer graph of every batch size now, not on first use
+        for (int n = 1; n <= cap; ++n) answer_graph(*s, *L.ws, n, nullptr);
     }
     via_service* raw = v.get();
     v->worker = std::thread([raw] { raw->run(); });
@@ -362,6 +364,16 @@ via_status via_service_stats_get(via_service* v, via_service_stats* out) {
 }
 
 void via_service_destroy(via_service* v) { delete v; }
+
+via_status via_service_stats_reset(via_service* v) {
+  if (!v) return fail(VIA_ERR_INVALID_ARGUMENT, "null argument");
+  std::lock_guard<std::mutex> lk(v->mu);
+  v->submitted = v->completed = v->failed = v->batches = v->units = 0;
+  v->max_in_flight = 0;
+  v->latencies.clear();
+  v->t_first = v->t_last = 0;
+  return VIA_OK;
+}
 
 uint64_t via_server_workspace_bytes(via_server* s, uint64_t max_queries) {
   if (!s || max_queries == 0 || max_queries > (1u << 20)) return 0;

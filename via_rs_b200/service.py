@@ -11,7 +11,7 @@ from .server import Server, check
 
 class ServiceConfig(ctypes.Structure):
     _fields_ = [("lanes", ctypes.c_uint32), ("max_batch", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
-                ("max_pending", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+                ("max_pending", ctypes.c_uint32), ("warm", ctypes.c_uint32)]
 
 
 class ServiceStats(ctypes.Structure):
@@ -39,6 +39,8 @@ def _bind():
     L.via_service_stats_get.argtypes = [vp, ctypes.POINTER(ServiceStats)]
     L.via_server_workspace_bytes.restype = ctypes.c_uint64
     L.via_server_workspace_bytes.argtypes = [vp, ctypes.c_uint64]
+    L.via_service_stats_reset.restype = ctypes.c_int
+    L.via_service_stats_reset.argtypes = [vp]
     L.via_service_destroy.restype = None
     L.via_service_destroy.argtypes = [vp]
     L._service_bound = True
@@ -56,11 +58,11 @@ class Service:
     poll()/wait() return its (mask, body) answer."""
 
     def __init__(self, server: Server, lanes: int = 2, max_batch: int = 64, hbm_budget: int = 0,
-                 max_pending: int = 0):
+                 max_pending: int = 0, warm: bool = False):
         self.server = server
         self.prm = server.prm
         L = _bind()
-        cfg = ServiceConfig(lanes, max_batch, hbm_budget, max_pending, 0)
+        cfg = ServiceConfig(lanes, max_batch, hbm_budget, max_pending, 1 if warm else 0)
         h = ctypes.c_void_p()
         check(L.via_service_create(server._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
@@ -92,6 +94,9 @@ class Service:
         st = ServiceStats()
         check(_bind().via_service_stats_get(self._h, ctypes.byref(st)))
         return {f: getattr(st, f) for f, _ in ServiceStats._fields_ if f != "reserved"}
+
+    def reset_stats(self) -> None:
+        check(_bind().via_service_stats_reset(self._h))
 
     def close(self) -> None:
         if getattr(self, "_h", None):
