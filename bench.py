@@ -206,6 +206,18 @@ def config_dict(prm):
 # ---------------------------------------------------------------------------
 # GPU arm.
 # ---------------------------------------------------------------------------
+def max_over_ranks(seconds, dist, device):
+    """The job's time: the slowest rank's (replicas run in parallel; the job ends
+    with the last one). Every rank calls this at the same point."""
+    if dist is None:
+        return seconds
+    import torch
+
+    t = torch.tensor([seconds], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def served_leg(args, prm, server, query, rate):
     """Seeded Poisson arrivals at `rate` requests/s into a 2-lane service; returns
     throughput and the service's p50/p99 submit-to-answer latency."""
@@ -345,10 +357,7 @@ def gpu_arm(args, prm):
     clk = clocks.stop()
     step_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     elapsed = evs[0].elapsed_time(evs[-1]) / 1e3
-    if dist:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(elapsed, dist, "cuda")
     n_answers = args.steps * world
     value = n_answers / elapsed
     db_bytes = prepared_db_bytes(prm)
@@ -363,10 +372,7 @@ def gpu_arm(args, prm):
     for _ in range(args.steps):
         server.answer(query)
     e2e_el = time.perf_counter() - t0
-    if dist:
-        t = torch.tensor([e2e_el], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_el = float(t.item())
+    e2e_el = max_over_ranks(e2e_el, dist, "cuda")
     e2e_value = n_answers / e2e_el
 
     # ---- batched: B independent queries per step share one database pass.
@@ -398,10 +404,7 @@ def gpu_arm(args, prm):
         torch.cuda.synchronize()
         b_ms = [bev[k].elapsed_time(bev[k + 1]) for k in range(kb)]
         b_el = bev[0].elapsed_time(bev[-1]) / 1e3
-        if dist:
-            t = torch.tensor([b_el], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            b_el = float(t.item())
+        b_el = max_over_ranks(b_el, dist, "cuda")
         b_value = kb * B * world / b_el
         batched = {"answers_s": b_value, "batch": B, "steps": kb, "ms_per_batch": b_el / kb * 1e3,
                    "db_gbs": b_value * db_bytes / 1e9 / B, "p50_ms": float(np.percentile(b_ms, 50)),
