@@ -6,7 +6,7 @@ reference's end-to-end property (the client recovers the queried record).
 import numpy as np
 import pytest
 
-from via_rs_b200.params import n8_preset, paper_preset, toy_preset
+from via_rs_b200.params import n8_preset, paper_preset, secure_preset, toy_preset
 from via_rs_b200.prg import Shake256Prg, nibble_records, seed_bytes
 from via_rs_b200.server import PublicKeys, QueryLengthMismatch, Server
 
@@ -180,3 +180,26 @@ def test_first_dim_matches_oracle_multi_tile(oracle):
     d_out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
     gpu.first_dim_dev(d_in.data_ptr(), d_out.data_ptr())
     assert np.array_equal(d_out.cpu().numpy().view(np.uint64), want)
+
+
+@pytest.mark.parametrize("stage", [1, 2, 3, 4, 5, 6, 7])
+def test_secure_preset_stage_parity(oracle, stage):
+    """SECURE_PARAMS (n1 = 4096): every intermediate equals the oracle's."""
+    prm = secure_preset(2, 4)
+    rng = np.random.default_rng(40 + stage)
+    records = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client, gpu, cpu = _setup(oracle, prm, records, b"secure-stage")
+    q = client.query(int(rng.integers(prm.capacity)), b"secure-stage-q")
+    got = gpu.debug_stage(q, stage)
+    want = cpu.debug_stage(q, stage)
+    bad = np.nonzero(got != want)[0]
+    assert bad.size == 0, f"stage {stage}: {bad.size} residues differ, first at {bad[:8]}"
+
+
+def test_secure_preset_answers(oracle):
+    prm = secure_preset(4, 8)
+    rng = np.random.default_rng(4097)
+    records = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client, gpu, cpu = _setup(oracle, prm, records, b"secure-answer")
+    for idx in (0, int(rng.integers(prm.capacity))):
+        _check_answer(client, gpu, cpu, records, idx, b"secure-a-%d" % idx)

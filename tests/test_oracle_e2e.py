@@ -76,3 +76,17 @@ def test_query_length_mismatch(oracle):
     with pytest.raises(oracle.OracleError) as e:
         server.answer(q[: -prm.lwe_len])
     assert e.value.code == 3
+
+
+def test_secure_preset_recovers(oracle):
+    """SECURE_PARAMS (n1=4096, n2=1024, q4=2^15; client_server_e2e_secure.rs): recover == record."""
+    from via_rs_b200.params import secure_preset
+
+    prm = secure_preset(2, 2)
+    rng = np.random.default_rng(4096)
+    recs = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client = oracle.Client(prm, b"via-c-secure-e2e")
+    server = oracle.Server(prm, client.cascade_key, client.conv_key, client.rsk, recs)
+    for idx in (3, prm.capacity - 1):
+        mask, body = server.answer(client.query(idx, b"secure-q-%d" % idx))
+        assert (client.recover(mask, body) == recs[idx]).all(), idx

@@ -1,4 +1,5 @@
 // Batched negacyclic NTT kernels (shared-memory staged, radix-2, Shoup twiddles).
+#include <algorithm>
 #include <cstring>
 
 #include "ntt.cuh"
@@ -143,13 +144,19 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
   }
 }
 
+// Threads of one k_ntt_reg CTA: 256, or one segment's n/8 when that is more.
+template <int LOGN>
+__host__ __device__ constexpr int ntt_cta() {
+  return ((1 << LOGN) / 8) > NTT_THREADS ? ((1 << LOGN) / 8) : NTT_THREADS;
+}
+
 template <int LOGN, bool INV>
-__global__ void __launch_bounds__(NTT_THREADS) k_ntt_reg(u64* __restrict__ data, int nl, long segments, NttTable t0,
-                                                         NttTable t1) {
+__global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg(u64* __restrict__ data, int nl, long segments,
+                                                             NttTable t0, NttTable t1) {
   constexpr int n = 1 << LOGN;
-  constexpr int TPS = n / 8;              // threads per segment
-  constexpr int SPC = NTT_THREADS / TPS;  // segments per CTA
-  __shared__ u64 sm[NTT_THREADS * 8];
+  constexpr int TPS = n / 8;                    // threads per segment
+  constexpr int SPC = ntt_cta<LOGN>() / TPS;    // segments per CTA
+  __shared__ u64 sm[ntt_cta<LOGN>() * 8];
   const int seg_local = threadIdx.x / TPS;
   const int tid = threadIdx.x % TPS;
   const long seg = (long)blockIdx.x * SPC + seg_local;
@@ -206,7 +213,7 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
                    cudaStream_t st) {
   if (segments <= 0) return;
   int logn = __builtin_ctz((unsigned)n);
-  if (n < 2 || (n & (n - 1)) || logn > 11) throw CudaError(100, "ntt: degree must be a power of two in [2, 2048]");
+  if (n < 2 || (n & (n - 1)) || logn > 12) throw CudaError(100, "ntt: degree must be a power of two in [2, 4096]");
   if (logn <= 2) {
     unsigned blocks = (unsigned)((segments + 127) / 128);
     if (logn == 1) k_ntt_tiny<1, INV><<<blocks, 128, 0, st>>>(data, nl, segments, t0, t1);
@@ -214,11 +221,12 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
     VIA_LAUNCHED();
     return;
   }
-  long spc = NTT_THREADS / (n / 8);
+  const int cta = std::max(NTT_THREADS, n / 8);
+  long spc = cta / (n / 8);
   unsigned blocks = (unsigned)((segments + spc - 1) / spc);
   switch (logn) {
 #define VIA_NTT_CASE(LG) \
-  case LG: k_ntt_reg<LG, INV><<<blocks, NTT_THREADS, 0, st>>>(data, nl, segments, t0, t1); break;
+  case LG: k_ntt_reg<LG, INV><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1); break;
     VIA_NTT_CASE(3)
     VIA_NTT_CASE(4)
     VIA_NTT_CASE(5)
@@ -228,6 +236,7 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
     VIA_NTT_CASE(9)
     VIA_NTT_CASE(10)
     VIA_NTT_CASE(11)
+    VIA_NTT_CASE(12)
 #undef VIA_NTT_CASE
   }
   VIA_LAUNCHED();

@@ -659,7 +659,7 @@ __device__ __forceinline__ void mac96(Acc96& acc, u64 a, u64 b) {
 }
 
 template <int LOGN>
-__global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __restrict__ cur, u64* __restrict__ nxt,
+__global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fused(const u64* __restrict__ cur, u64* __restrict__ nxt,
                                                                   KeySel ks, DevRing R, Gadget g) {
   constexpr int n = 1 << LOGN;
   using In0 = NttPhase<LOGN, true, 0>;
@@ -743,12 +743,13 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_cmux_fused(const u64* __
 // supported degree and a small gadget, else diff -> external product -> add.
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
   return R.ntt && R.nl == 1 && g.small && g.S < ((u128)1 << 32) && R.m[0].q < (1ull << 40) &&
-         (R.n == 2048 || R.n == 1024 || R.n == 512);
+         (R.n == 4096 || R.n == 2048 || R.n == 1024 || R.n == 512);
 }
 
 static void cmux_fused(const DevRing& R, const Gadget& g, const u64* cur, u64* nxt, KeySel ks, long count,
                        cudaStream_t st) {
   switch (R.n) {
+    case 4096: k_cmux_fused<12><<<(unsigned)count, 512, 0, st>>>(cur, nxt, ks, R, g); break;
     case 2048: k_cmux_fused<11><<<(unsigned)count, 256, 0, st>>>(cur, nxt, ks, R, g); break;
     case 1024: k_cmux_fused<10><<<(unsigned)count, 128, 0, st>>>(cur, nxt, ks, R, g); break;
     default: k_cmux_fused<9><<<(unsigned)count, 64, 0, st>>>(cur, nxt, ks, R, g); break;

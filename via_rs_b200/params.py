@@ -150,6 +150,20 @@ def paper_preset(num_rows: int = 256, num_cols: int = 4096, n_rec: int = 512) ->
     )
 
 
+SECURE_Q1 = (173_964_607_489, 173_964_656_641)
+
+
+def secure_preset(num_rows: int = 256, num_cols: int = 4096, n_rec: int = 1024) -> Params:
+    """SECURE_PARAMS (crates/via-protocol/src/presets.rs:278-303): the >= 120-bit
+    VIA-C preset, n1=4096, n2=1024, q1 two 38-bit primes, q4=2^15, erratum gadgets."""
+    return Params(
+        n1=4096, n2=1024, n_rec=n_rec, num_rows=num_rows, num_cols=num_cols,
+        q1=SECURE_Q1, q2=PAPER_Q2, q3=PAPER_Q3, q4=1 << 15, p=16,
+        b_dmux=18073, b_cmux=307, ck_base=18, b_rsk=4,
+        l_query=2, l_ck=18, l_rsk=8,
+    )
+
+
 def toy_preset(num_rows: int = 16, num_cols: int = 16, n_rec: int = 16) -> Params:
     """TOY_PARAMS; 1024 records of 16 4-bit coefficients at I=J=16."""
     return Params(
