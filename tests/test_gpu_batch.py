@@ -45,3 +45,20 @@ def test_answer_batch_rejects_wrong_sizes(oracle):
         gpu.answer_batch(qs[:4])
     with pytest.raises(QueryLengthMismatch):
         gpu.answer_batch(qs[:, : -prm.lwe_len])
+
+
+def test_answer_batch_t256_recovers(oracle):
+    """The production VIA-B batch: T = 256 records of degree 2 per answer (depth-10
+    repack). The oracle would take minutes for 256 queries, so the check is the
+    reference's e2e property: recover_batch returns every queried record."""
+    prm = paper_preset(2, 2, n_rec=2)
+    assert prm.n2 // prm.n_rec == 256
+    rng = np.random.default_rng(256)
+    recs = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
+    client = oracle.Client(prm, b"gpu-via-b-t256")
+    gpu = Server.setup(prm, PublicKeys(client.cascade_key, client.conv_key, client.rsk), recs)
+    idx = [int(i) for i in rng.integers(prm.capacity, size=256)]
+    gm, gb = gpu.answer_batch(client.batch_query(idx, b"t256"))
+    got = client.recover_batch(gm, gb)
+    bad = [t for t, i in enumerate(idx) if not np.array_equal(got[t], recs[i])]
+    assert not bad, f"{len(bad)} of 256 records wrong, first slots {bad[:8]}"
