@@ -265,6 +265,24 @@ via_status via_service_stats_reset(via_service* v);
 void via_service_destroy(via_service* v);
 
 /*
+ * Query wire formats (via-protocol/src/wire/format.rs:93-190). A wire query is
+ * n_lwe packets, one per LWE, each led by the format tag:
+ *   0x00 Uncompressed : [0x00][count u64 LE = nl*(n1+1)][the LWE's u64s, LE]
+ *   0x01 PrgCompressed: [0x01][seed, 32 bytes][count u64 LE = nl][the body's u64s, LE]
+ * A compressed packet's mask is regenerated as Shake256Prg(seed).uniform_below(q_l),
+ * row-major, one draw per limb, limb 0 first (format.rs:20-27); the device
+ * computes the PRG blocks in parallel. Errors: VIA_ERR_UNKNOWN_FORMAT_TAG,
+ * VIA_ERR_BUFFER_TOO_SHORT (truncated or too few packets),
+ * VIA_ERR_QUERY_LENGTH_MISMATCH (bytes after the last packet),
+ * VIA_ERR_DIM_MISMATCH (a packet's count does not match the parameters).
+ */
+via_status via_query_from_wire(via_server* s, const uint8_t* wire, uint64_t len, uint64_t* out_query,
+                               uint64_t out_len);
+/* Decodes a wire query on the device and answers it (host answer buffers). */
+via_status via_server_answer_wire(via_server* s, const uint8_t* wire, uint64_t len, uint64_t* out_mask,
+                                  uint64_t* out_body);
+
+/*
  * The FirstDim scan of via_first_dim_scan_dev for callers that cannot allocate
  * device memory: code that runs where cudaMalloc is not allowed or not wanted
  * (inside a region being captured into a CUDA graph, a host whose allocator is

@@ -61,6 +61,12 @@ def lib() -> ctypes.CDLL:
     L.via_server_answer_batch_dev.restype = ctypes.c_int
     L.via_server_answer_batch_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_uint64,
                                               ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_query_from_wire.restype = ctypes.c_int
+    L.via_query_from_wire.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                      ctypes.c_uint64]
+    L.via_server_answer_wire.restype = ctypes.c_int
+    L.via_server_answer_wire.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
+                                         ctypes.c_void_p]
     L.via_first_dim_scan_many_dev.restype = ctypes.c_int
     L.via_first_dim_scan_many_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_void_p,
                                               ctypes.c_void_p]
