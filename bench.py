@@ -60,6 +60,7 @@ def parse():
     ap.add_argument("--served", type=int, default=384,
                     help="requests of the served leg (Poisson arrivals, continuous batching; 0 = skip)")
     ap.add_argument("--via-b", type=int, default=1, help="run the VIA-B leg (T = 8, records of degree 64)")
+    ap.add_argument("--no-autotune", action="store_true", help="keep the default scan tiles (skip the autotuner)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="set up, answer one batch of --batch queries and exit (a short target for ncu)")
     return ap.parse_args()
@@ -225,7 +226,9 @@ def served_leg(args, prm, server, query, rate):
 
     rng = np.random.default_rng(7)
     gaps = rng.exponential(1.0 / rate, size=args.served)
-    svc = Service(server, lanes=2, max_batch=64, warm=True)  # graphs of every batch size captured up front
+    # Scan tiles tuned for batch sizes 1, 2, 4, ..., 64 and the graphs of every
+    # batch size captured up front.
+    svc = Service(server, lanes=2, max_batch=64, warm=True, autotune=not args.no_autotune)
     try:
         for t in [svc.submit(query) for _ in range(4)]:
             svc.wait(t)
@@ -242,12 +245,14 @@ def served_leg(args, prm, server, query, rate):
             svc.wait(t)
         wall = time.perf_counter() - t0
         st = svc.stats()
+        tuning = svc.tuning()
     finally:
         svc.close()
     return {"requests": args.served, "offered_rate_hz": rate, "answers_s": st["answers_per_s"],
             "wall_answers_s": args.served / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
             "mean_batch": st["mean_batch"], "batches": st["batches"], "lanes": st["lanes"],
-            "max_in_flight": st["max_in_flight"], "arrivals": "seeded Poisson (numpy PCG64 seed 7)"}
+            "max_in_flight": st["max_in_flight"], "arrivals": "seeded Poisson (numpy PCG64 seed 7)",
+            "scan_tiles": [{"batch": e["batch"], **e["tile"]} for e in tuning]}
 
 
 def via_b_leg(args, prm, rank):
@@ -322,6 +327,11 @@ def gpu_arm(args, prm):
     def answer_dev():
         check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr()), prm.n_lwe,
                                       ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()), sptr))
+
+    # Scan autotuner: the fastest tile for one query and for the batched leg.
+    tuning = []
+    if not args.no_autotune:
+        tuning = server.autotune([1] + ([args.batch] if args.batch > 1 else []))
 
     if args.profile_batch:
         B = max(1, args.batch)
@@ -459,6 +469,7 @@ def gpu_arm(args, prm):
                          "launch_ms": scan_s * 1e3, "algorithmic_bytes": scan_bytes},
             "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
                     "d2h_bytes_per_step": int(2 * prm.n2 * 8)},
+            "autotune": tuning,
             "gpu_launches": int(launches),
             "clocks": clk,
         }

@@ -183,6 +183,47 @@ via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, 
                                        uint64_t* out_eval, void* stream);
 
 /*
+ * Scan autotuner. The FirstDim scan (`first_dim`, first_dim.rs:94-184, run as a
+ * tensor-core integer GEMM) has a tile space: selection columns per tile for
+ * batches, the depth of its shared-memory ring, and the order its persistent
+ * CTAs walk the (slot, column-tile) units in. Every tile gives the same exact
+ * result. via_server_autotune times every candidate tile for each listed batch
+ * size on this server's database (CUDA events, one warm-up and three timed
+ * scans each) and keeps the fastest; scans of other batch sizes use the entry
+ * of the nearest tuned size above (else below) of the same kind (one query, or
+ * a batch). With a cache_path, entries measured before for the same device,
+ * ring degree, grid and modulus are read from that file instead of measured,
+ * and new measurements are appended to it. Answer graphs captured before the
+ * call are re-captured on next use. Servers on non-NTT rings have no tiles:
+ * their entries report 0 candidates. `out` (may be NULL) receives one entry
+ * per batch size. No counterpart in the reference, whose FirstDim is a
+ * threaded CPU loop.
+ */
+typedef struct via_scan_tile {
+  uint32_t n_max;    /* selection columns per tile for batches: 16, 32 or 48; 0 = default (48) */
+  uint32_t stages;   /* shared-memory ring depth, 2..6; 0 = default (3; 4 for one query) */
+  uint32_t order;    /* 0: slot-major units, 1: tile-major units (batches only) */
+  uint32_t reserved;
+} via_scan_tile;
+
+typedef struct via_scan_tuning {
+  uint32_t batch;       /* queries per scan */
+  via_scan_tile tile;   /* the tile kept */
+  float ms;             /* its scan time in milliseconds */
+  float default_ms;     /* the default tile's scan time */
+  uint32_t candidates;  /* tiles measured; 0 when read from the cache file */
+  uint32_t reserved;
+} via_scan_tuning;
+
+via_status via_server_autotune(via_server* s, const uint32_t* batch_sizes, uint64_t count, const char* cache_path,
+                               via_scan_tuning* out);
+/* Sets (tile != NULL) or clears the tile used for scans of `batch` queries. */
+via_status via_server_set_scan_tile(via_server* s, uint32_t batch, const via_scan_tile* tile);
+/* The candidate tiles for `batch` queries (the default first); returns their
+ * number and writes up to `cap` of them to `out` (may be NULL). */
+uint64_t via_scan_tile_candidates(via_server* s, uint32_t batch, via_scan_tile* out, uint64_t cap);
+
+/*
  * Runs the answer up to `stage` and copies that stage's output, in coefficient
  * form, to the host buffer `out` (for stage-by-stage parity checks):
  *   1 cascade RLWEs [n_lwe][2][nl][n1]      (query_decomp.rs:76-78)
@@ -233,6 +274,9 @@ typedef struct {
   uint64_t hbm_budget;  /* device bytes for all lanes' workspaces; 0 -> max_batch decides */
   uint32_t max_pending; /* queued requests before submit returns VIA_ERR_BUSY; 0 -> 2^20 */
   uint32_t warm;        /* nonzero: capture every batch size's answer graph at creation */
+  uint32_t autotune;    /* nonzero: run the scan autotuner (via_server_autotune) at creation
+                           for the batch sizes 1, 2, 4, ... up to the lane capacity */
+  const char* tune_cache; /* the autotuner's cache file, or NULL */
 } via_service_config;
 
 typedef struct {
@@ -261,6 +305,9 @@ via_status via_service_wait(via_service* v, uint64_t ticket, uint64_t* out_mask,
 via_status via_service_stats_get(via_service* v, via_service_stats* out);
 /* Zeroes the counters and latency record (requests in flight still complete). */
 via_status via_service_stats_reset(via_service* v);
+/* The autotuner's choices made at creation (cfg.autotune): returns their
+ * number and writes up to `cap` entries to `out` (may be NULL). */
+uint64_t via_service_tuning(via_service* v, via_scan_tuning* out, uint64_t cap);
 /* Finishes the batches on the GPU, drops queued requests, frees the lanes. */
 void via_service_destroy(via_service* v);
 

@@ -21,6 +21,25 @@ class ViaPublicKeys(ctypes.Structure):
     _fields_ = [("cascade_key", _u64p), ("conv_key", _u64p), ("rsk", _u64p)]
 
 
+class ScanTile(ctypes.Structure):
+    """via_scan_tile: one FirstDim scan tile choice."""
+    _fields_ = [("n_max", ctypes.c_uint32), ("stages", ctypes.c_uint32), ("order", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {"n_max": self.n_max, "stages": self.stages, "order": self.order}
+
+
+class ScanTuning(ctypes.Structure):
+    """via_scan_tuning: the autotuner's choice for one batch size."""
+    _fields_ = [("batch", ctypes.c_uint32), ("tile", ScanTile), ("ms", ctypes.c_float), ("default_ms", ctypes.c_float),
+                ("candidates", ctypes.c_uint32), ("reserved", ctypes.c_uint32)]
+
+    def as_dict(self) -> dict:
+        return {"batch": self.batch, "tile": self.tile.as_dict(), "ms": round(float(self.ms), 4),
+                "default_ms": round(float(self.default_ms), 4), "candidates": self.candidates}
+
+
 def declared_symbols() -> list:
     """Function names declared in include/via_gpu.h."""
     text = HEADER.read_text()
@@ -81,6 +100,14 @@ def lib() -> ctypes.CDLL:
     L.via_server_reserve.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
     L.via_first_dim_scan_static.restype = ctypes.c_int
     L.via_first_dim_scan_static.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
+    L.via_server_autotune.restype = ctypes.c_int
+    L.via_server_autotune.argtypes = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_uint32), ctypes.c_uint64,
+                                      ctypes.c_char_p, ctypes.POINTER(ScanTuning)]
+    L.via_server_set_scan_tile.restype = ctypes.c_int
+    L.via_server_set_scan_tile.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ScanTile)]
+    L.via_scan_tile_candidates.restype = ctypes.c_uint64
+    L.via_scan_tile_candidates.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ScanTile),
+                                           ctypes.c_uint64]
     L.via_kernel_launches.restype = ctypes.c_uint64
     L.via_kernel_launches.argtypes = []
     _lib = L

@@ -37,7 +37,7 @@ struct KParams {
   u64* out;
   int* err;
   int n, J, n_jt, n_kc, n_ct, N, Np, nq;
-  int stages, grouped, acc_stride, nacc, tmem_cols;
+  int stages, grouped, acc_stride, nacc, tmem_cols, order;
   DevMod m;
 };
 
@@ -140,6 +140,17 @@ __device__ __forceinline__ void pin(u32 (&r)[K]) {
   for (int x = 0; x < K; ++x) asm volatile("" : "+r"(r[x]));
 }
 
+// Work unit u -> (slot t, c-tile ct) in the tile's order.
+__device__ __forceinline__ void unit_coords(const KParams& P, int u, int& t, int& ct) {
+  if (P.order) {
+    t = u % P.n;
+    ct = u / P.n;
+  } else {
+    t = u / P.n_ct;
+    ct = u % P.n_ct;
+  }
+}
+
 // sum_g v_g 2^{8g} mod q for nine group sums v_g < 2^31.
 __device__ __forceinline__ u64 fold9(const u32 (&v)[9], const DevMod& m) {
   const u64 lo = (u64)v[0] + ((u64)v[1] << 8) + ((u64)v[2] << 16) + ((u64)v[3] << 24);
@@ -201,7 +212,8 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
       u32 armed = 0, armed_par = 0;  // per stage: armed at least once; parity of its last armed phase
       bool ok = true;
       for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
-        const int t = u / P.n_ct, ct = u % P.n_ct;
+        int t, ct;
+        unit_coords(P, u, t, ct);
         const uint8_t* selu = P.sel + ((size_t)t * P.n_ct + ct) * P.n_kc * sel_chunk;
         const uint8_t* dbt = P.db + (size_t)t * P.n_jt * P.n_kc * FD_CHUNK;
         for (int jt = 0; ok && jt < P.n_jt; ++jt)
@@ -300,7 +312,8 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
     u32 aph = 0;
     bool ok = true;
     for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
-      const int t = u / P.n_ct, ct = u % P.n_ct;
+      int t, ct;
+      unit_coords(P, u, t, ct);
       for (int jt = 0; jt < P.n_jt; ++jt) {
         // Warp-uniform: the TMEM loads below are .sync.aligned.
         if (!__all_sync(0xffffffffu, mbar_wait(acc_full + a, aph, abort_flag))) {
@@ -442,11 +455,11 @@ __global__ void k_fd_planes(const u64* __restrict__ stage, int i0, int I, int J,
 }
 
 struct Tiling {
-  int grouped, N, Np, n_ct, stages, acc_stride, nacc, tmem_cols;
+  int grouped, N, Np, n_ct, stages, acc_stride, nacc, tmem_cols, order;
   size_t smem;
 };
 
-Tiling tiling(int nq) {
+Tiling tiling(int nq, const FdTile& tile) {
   Tiling T{};
   int acc_cols;
   if (nq == 1) {
@@ -454,14 +467,17 @@ Tiling tiling(int nq) {
     T.N = 2;
     T.Np = 16;
     T.n_ct = 1;
-    T.stages = 4;
+    T.stages = tile.stages ? tile.stages : 4;
+    T.order = 0;
     acc_cols = 16 * FD_LIMBS;
   } else {
+    const int cap = tile.n_max ? tile.n_max : 48;
     T.grouped = 1;
-    T.n_ct = (2 * nq + 47) / 48;
+    T.n_ct = (2 * nq + cap - 1) / cap;
     T.N = fd_round_up((2 * nq + T.n_ct - 1) / T.n_ct, 16);
     T.Np = FD_LIMBS * T.N;
-    T.stages = 3;
+    T.stages = tile.stages ? tile.stages : 3;
+    T.order = tile.order;
     acc_cols = 9 * T.N;
   }
   T.acc_stride = fd_round_up(acc_cols, 32);
@@ -473,6 +489,9 @@ Tiling tiling(int nq) {
   return T;
 }
 
+// The built-in shared-memory limit the kernel was first tuned under.
+constexpr int SMEM_DEFAULT = 200 * 1024;
+
 }  // namespace
 
 size_t fd_planes_bytes(int I, int J, int n) {
@@ -480,6 +499,60 @@ size_t fd_planes_bytes(int I, int J, int n) {
 }
 
 bool fd_supported(int I, int n, u64 q) { return I >= 1 && I <= 4096 && n >= 1 && q < (1ull << 40); }
+
+bool fd_tile_valid(const FdPlan& p, int nq, const FdTile& t) {
+  if (nq < 1) return false;
+  if (t.n_max != 0 && t.n_max != 16 && t.n_max != 32 && t.n_max != 48) return false;
+  if (t.stages != 0 && (t.stages < 2 || t.stages > 6)) return false;
+  if (t.order != 0 && t.order != 1) return false;
+  if (nq == 1 && (t.n_max != 0 || t.order != 0)) return false;
+  const Tiling T = tiling(nq, t);
+  const size_t limit = p.smem_max > 0 ? (size_t)p.smem_max : (size_t)SMEM_DEFAULT;
+  return T.Np <= 256 && T.nacc * T.acc_stride <= 512 && T.smem <= limit;
+}
+
+FdTile fd_tile_for(const FdPlan& p, int nq) {
+  const FdTile* below = nullptr;
+  for (const auto& e : p.tuned) {
+    if ((e.first == 1) != (nq == 1)) continue;  // one-query and batch tiles do not mix
+    if (e.first >= nq) return fd_tile_valid(p, nq, e.second) ? e.second : FdTile{};
+    below = &e.second;
+  }
+  return below && fd_tile_valid(p, nq, *below) ? *below : FdTile{};
+}
+
+void fd_set_tile(FdPlan& p, int nq, const FdTile& t) {
+  for (auto& e : p.tuned)
+    if (e.first == nq) {
+      e.second = t;
+      return;
+    }
+  p.tuned.push_back({nq, t});
+  std::sort(p.tuned.begin(), p.tuned.end(),
+            [](const std::pair<int, FdTile>& a, const std::pair<int, FdTile>& b) { return a.first < b.first; });
+}
+
+std::vector<FdTile> fd_tile_candidates(const FdPlan& p, int nq) {
+  std::vector<FdTile> out;
+  out.push_back(FdTile{});  // the default first
+  auto add = [&](FdTile t) {
+    const Tiling a = tiling(nq, t);
+    if (!fd_tile_valid(p, nq, t)) return;
+    for (const FdTile& o : out) {  // skip tiles that launch the same kernel configuration
+      const Tiling b = tiling(nq, o);
+      if (a.N == b.N && a.n_ct == b.n_ct && a.stages == b.stages && a.order == b.order) return;
+    }
+    out.push_back(t);
+  };
+  if (nq == 1) {
+    for (int st = 2; st <= 6; ++st) add(FdTile{0, st, 0});
+  } else {
+    for (int nm : {16, 32, 48})
+      for (int st = 2; st <= 5; ++st)
+        for (int od = 0; od <= 1; ++od) add(FdTile{nm, st, od});
+  }
+  return out;
+}
 
 void fd_rows_to_planes(const u64* stage, int i0, const FdPlan& p, uint8_t* planes, cudaStream_t st) {
   const long total = (long)p.J * p.n;
@@ -489,16 +562,29 @@ void fd_rows_to_planes(const u64* stage, int i0, const FdPlan& p, uint8_t* plane
 }
 
 size_t fd_sel_bytes(const FdPlan& p, int nq) {
-  Tiling T = tiling(nq);
-  return (size_t)p.n * T.n_ct * (size_t)T.Np * p.I_pad;
+  // Every candidate's split selection: n * n_ct * Np * I_pad bytes.
+  size_t bytes = 0;
+  for (const FdTile& t : fd_tile_candidates(p, nq)) {
+    const Tiling T = tiling(nq, t);
+    bytes = std::max(bytes, (size_t)p.n * T.n_ct * (size_t)T.Np * p.I_pad);
+  }
+  return bytes;
 }
 
-void fd_prepare_device() {
-  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024));
+int fd_prepare_device() {
+  int dev = 0, optin = 0;
+  VIA_CUDA(cudaGetDevice(&dev));
+  VIA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  const int limit = std::max(optin, SMEM_DEFAULT);
+  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  return limit;
 }
 
-void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st) {
-  const Tiling T = tiling(nq);
+void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st,
+             const FdTile* force) {
+  const FdTile tile = force ? *force : fd_tile_for(p, nq);
+  if (force && !fd_tile_valid(p, nq, tile)) throw CudaError(100, "scan tile not valid for this batch");
+  const Tiling T = tiling(nq, tile);
   const int n_k16 = p.I_pad / 16, n_kc = p.I_pad / FD_KC;
   const long total = (long)p.n * T.n_ct * T.N * n_k16;
   k_fd_split<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(sel_eval, nq, p.I, p.n, n_k16, n_kc, T.n_ct, T.N, T.Np,
@@ -522,11 +608,39 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
   K.acc_stride = T.acc_stride;
   K.nacc = T.nacc;
   K.tmem_cols = T.tmem_cols;
+  K.order = T.order;
   K.m = p.m;
   const int units = p.n * T.n_ct;
   const int grid = std::min(units, p.grid);
   k_fd_tc<<<grid, FD_THREADS, T.smem, st>>>(K);
   VIA_LAUNCHED();
+}
+
+std::vector<FdTuneResult> fd_measure_tiles(const FdPlan& p, int nq, const u64* sel_eval, u64* out_eval,
+                                           uint8_t* scratch, cudaStream_t st, int reps) {
+  std::vector<FdTuneResult> out;
+  cudaEvent_t e0, e1;
+  VIA_CUDA(cudaEventCreate(&e0));
+  VIA_CUDA(cudaEventCreate(&e1));
+  try {
+    for (const FdTile& t : fd_tile_candidates(p, nq)) {
+      fd_scan(p, sel_eval, out_eval, nq, scratch, st, &t);  // warm-up
+      VIA_CUDA(cudaEventRecord(e0, st));
+      for (int r = 0; r < reps; ++r) fd_scan(p, sel_eval, out_eval, nq, scratch, st, &t);
+      VIA_CUDA(cudaEventRecord(e1, st));
+      VIA_CUDA(cudaEventSynchronize(e1));
+      float ms = 0.f;
+      VIA_CUDA(cudaEventElapsedTime(&ms, e0, e1));
+      out.push_back(FdTuneResult{t, ms / (float)std::max(1, reps)});
+    }
+  } catch (...) {
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    throw;
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  return out;
 }
 
 }  // namespace via

@@ -11,6 +11,8 @@
 #pragma once
 #include <cstddef>
 #include <cstdint>
+#include <utility>
+#include <vector>
 
 #include "common.cuh"
 
@@ -26,32 +28,74 @@ constexpr int FD_MT = 128;    // database columns per MMA tile (the M dimension)
 constexpr int FD_LIMBS = 5;   // bytes per residue
 constexpr int FD_CHUNK = FD_LIMBS * FD_MT * FD_KC;  // 40960 bytes
 
+// One scan tile choice, the autotuner's search space. Every choice computes the
+// same exact sums; they differ in speed only.
+//  n_max  : selection columns per c-tile for batches (16, 32 or 48); the
+//           batch's 2*nq columns are spread evenly over ceil(2nq / n_max)
+//           tiles, each padded to a multiple of 16. Ignored for one query.
+//  stages : depth of the shared-memory ring of (database, selection) chunks.
+//  order  : 0 walks units slot-major (the c-tiles of one slot run on
+//           neighbouring SMs at the same time and share the slot's planes in
+//           L2); 1 walks them tile-major (one c-tile over every slot, then the next).
+// Zero fields take the built-in default (48 columns, 3 stages; 4 for one query).
+struct FdTile {
+  int n_max = 0, stages = 0, order = 0;
+};
+
 struct FdPlan {
   const uint8_t* planes = nullptr;
   int I = 0, J = 0, n = 0;  // rows, columns, ring degree
   int I_pad = 0, J_pad = 0;
   DevMod m{};
-  int grid = 148;  // persistent CTAs (one per SM)
-  int* err = nullptr;  // device word: nonzero after a bounded wait ran out
+  int grid = 148;          // persistent CTAs (one per SM)
+  int smem_max = 0;        // opt-in shared memory per block on this device
+  int* err = nullptr;      // device word: nonzero after a bounded wait ran out
+  // Tuned tiles by batch size, sorted by batch. A scan of nq queries uses the
+  // entry of the smallest tuned batch >= nq of the same kind (one query or a
+  // batch), else the largest below it, else the default.
+  std::vector<std::pair<int, FdTile>> tuned;
 };
 
 inline int fd_round_up(int v, int a) { return (v + a - 1) / a * a; }
 size_t fd_planes_bytes(int I, int J, int n);
 bool fd_supported(int I, int n, u64 q);
 
+// The tile a scan of nq queries runs with (tuned entry or default).
+FdTile fd_tile_for(const FdPlan& p, int nq);
+// Every tile the autotuner tries for nq queries (all valid on this device).
+std::vector<FdTile> fd_tile_candidates(const FdPlan& p, int nq);
+bool fd_tile_valid(const FdPlan& p, int nq, const FdTile& t);
+// Records `t` as the tile for batches of nq (replacing an entry for nq).
+void fd_set_tile(FdPlan& p, int nq, const FdTile& t);
+
+struct FdTuneResult {
+  FdTile tile;
+  float ms = 0.f;
+};
+// Times every candidate tile for nq queries on the given buffers (their
+// contents are irrelevant to the timing and are overwritten): one warm-up scan
+// and `reps` timed scans each, with CUDA events on `st`. Returns the
+// measurements in candidate order; the first entry is the default tile.
+std::vector<FdTuneResult> fd_measure_tiles(const FdPlan& p, int nq, const u64* sel_eval, u64* out_eval,
+                                           uint8_t* scratch, cudaStream_t st, int reps);
+
 // Converts rows [i0, i0 + 16) of an eval-form database held as u64 [16][J][n]
 // (`stage`, rows beyond I ignored) into the byte planes.
 void fd_rows_to_planes(const u64* stage, int i0, const FdPlan& p, uint8_t* planes, cudaStream_t st);
 
-// Raises the scan kernel's shared-memory limit on the current device (once per
-// device, before the first fd_scan there).
-void fd_prepare_device();
+// Raises the scan kernel's shared-memory limit on the current device to the
+// device's opt-in maximum (once per device, before the first fd_scan there) and
+// returns that maximum in bytes.
+int fd_prepare_device();
 
-// Scratch (bytes) that fd_scan needs for nq queries' split selection vectors.
+// Scratch (bytes) that fd_scan needs for nq queries' split selection vectors,
+// whichever candidate tile the scan runs with.
 size_t fd_sel_bytes(const FdPlan& p, int nq);
 
 // out_eval[b][j] = sum_i sel_eval[b][i] (.) db[i][j] for mask and body:
-// sel_eval [nq][I][2][n], out_eval [nq][J][2][n], eval form mod q2.
-void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st);
+// sel_eval [nq][I][2][n], out_eval [nq][J][2][n], eval form mod q2. `force`
+// overrides the tuned tile (it must be valid for nq).
+void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st,
+             const FdTile* force = nullptr);
 
 }  // namespace via

@@ -426,6 +426,7 @@ struct Workspace {
   std::vector<std::pair<int, unsigned long long>> graph_kernels;
   std::unique_ptr<struct RepackWs> repack;  // VIA-B buffers, made on the first batch answer
   cudaStream_t capture = nullptr;           // stream the answer graphs are captured on
+  int graphs_gen = 0;                       // Server::plan_gen the graphs were captured under
   ~Workspace() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     if (capture) cudaStreamDestroy(capture);
@@ -445,6 +446,13 @@ void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, ui
   for (int q = 0; q < nq; ++q)
     first_dim_schoolbook(s.db.p, sel_eval + (size_t)q * p.num_rows * 2 * p.n1, out_eval + (size_t)q * p.num_cols * 2 * p.n1,
                          (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], st);
+}
+
+// Times every candidate scan tile for nq queries on the handle's workspace
+// buffers (the workspace must hold batches of nq).
+std::vector<FdTuneResult> workspace_measure_tiles(Server& s, Workspace& w, int nq, int reps) {
+  if (w.bmax < nq) throw CudaError(100, "workspace smaller than the batch to tune");
+  return fd_measure_tiles(s.fd, nq, w.sel.p, w.fd_out.p, reinterpret_cast<uint8_t*>(w.sel_bytes.p), s.stream, reps);
 }
 
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g);
@@ -963,6 +971,12 @@ u64* workspace_answer_body(Server& s) { return s.ws->a_body.p; }
 void answer_graph(Server& s, Workspace& w, int nq, cudaStream_t st) {
   cudaGraphExec_t exec = nullptr;
   unsigned long long kernels = 0;
+  if (w.graphs_gen != s.plan_gen) {  // the scan tiles changed since these were captured
+    for (auto& g : w.graphs) cudaGraphExecDestroy(g.second);
+    w.graphs.clear();
+    w.graph_kernels.clear();
+    w.graphs_gen = s.plan_gen;
+  }
   for (size_t i = 0; i < w.graphs.size(); ++i)
     if (w.graphs[i].first == nq) {
       exec = w.graphs[i].second;

@@ -1,4 +1,6 @@
 // Server::setup / answer / destroy behind the C ABI of include/via_gpu.h.
+#include <algorithm>
+#include <cstdio>
 #include <cstring>
 #include <mutex>
 #include <string>
@@ -232,7 +234,7 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     s.fd.J_pad = fd_round_up((int)J, FD_MT);
     s.fd.m = s.r2.m[0];
     VIA_CUDA(cudaDeviceGetAttribute(&s.fd.grid, cudaDevAttrMultiProcessorCount, s.device));
-    fd_prepare_device();
+    s.fd.smem_max = fd_prepare_device();
     s.planes.alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1) / 8);
     VIA_CUDA(cudaMemsetAsync(s.planes.p, 0, s.planes.n * 8, s.stream));
     s.fd_err.alloc(1);
@@ -448,6 +450,158 @@ via_status via_server_reserve(via_server* s, uint64_t max_queries) {
     std::lock_guard<std::mutex> g(s->mu);
     ensure_batch(s, max_queries);
   });
+}
+
+}  // extern "C"
+
+namespace via {
+// ---------------------------------------------------------------------------
+// Scan autotuner: measures every candidate tile of the FirstDim scan for the
+// given batch sizes on this server's database and keeps the fastest. A cache
+// file (one line per measured configuration, keyed by device name, ring degree,
+// grid and modulus) lets later processes skip the measurement.
+namespace {
+
+std::string tune_key(const Server& s, int nq) {
+  cudaDeviceProp prop{};
+  VIA_CUDA(cudaGetDeviceProperties(&prop, s.device));
+  std::string dev = prop.name;
+  for (char& c : dev)
+    if (c == ' ' || c == '\t') c = '_';
+  return "fd_tc/1 " + dev + " n=" + std::to_string(s.fd.n) + " I=" + std::to_string(s.fd.I) +
+         " J=" + std::to_string(s.fd.J) + " q=" + std::to_string(s.fd.m.q) + " nq=" + std::to_string(nq);
+}
+
+struct CachedTile {
+  FdTile tile;
+  float ms = 0.f, default_ms = 0.f;
+};
+
+// Cache line: <key> | <n_max> <stages> <order> <ms> <default_ms>
+std::vector<std::pair<std::string, CachedTile>> read_tune_cache(const char* path) {
+  std::vector<std::pair<std::string, CachedTile>> out;
+  if (!path || !*path) return out;
+  FILE* f = fopen(path, "r");
+  if (!f) return out;
+  char line[512];
+  while (fgets(line, sizeof line, f)) {
+    char* bar = strchr(line, '|');
+    if (!bar) continue;
+    std::string key(line, bar - line);
+    while (!key.empty() && key.back() == ' ') key.pop_back();
+    CachedTile c;
+    if (sscanf(bar + 1, "%d %d %d %f %f", &c.tile.n_max, &c.tile.stages, &c.tile.order, &c.ms, &c.default_ms) == 5)
+      out.push_back({key, c});
+  }
+  fclose(f);
+  return out;
+}
+
+void append_tune_cache(const char* path, const std::string& key, const CachedTile& c) {
+  if (!path || !*path) return;
+  FILE* f = fopen(path, "a");
+  if (!f) throw ApiError(VIA_ERR_INVALID_ARGUMENT, std::string("cannot append to the tuning cache ") + path);
+  fprintf(f, "%s | %d %d %d %.6f %.6f\n", key.c_str(), c.tile.n_max, c.tile.stages, c.tile.order, c.ms, c.default_ms);
+  fclose(f);
+}
+
+via_scan_tile to_abi(const FdTile& t) { return via_scan_tile{(uint32_t)t.n_max, (uint32_t)t.stages, (uint32_t)t.order, 0}; }
+FdTile from_abi(const via_scan_tile& t) { return FdTile{(int)t.n_max, (int)t.stages, (int)t.order}; }
+
+}  // namespace
+
+void autotune_scan(Server& s, Workspace& w, const std::vector<int>& sizes, const char* cache_path,
+                   std::vector<via_scan_tuning>* out) {
+  if (!s.tensor_fd()) {  // schoolbook rings have no tiles
+    if (out)
+      for (int nq : sizes) out->push_back(via_scan_tuning{(uint32_t)nq, {0, 0, 0, 0}, 0.f, 0.f, 0, 0});
+    return;
+  }
+  const auto cache = read_tune_cache(cache_path);
+  for (int nq : sizes) {
+    const std::string key = tune_key(s, nq);
+    const CachedTile* hit = nullptr;
+    for (const auto& e : cache)
+      if (e.first == key && fd_tile_valid(s.fd, nq, e.second.tile)) hit = &e.second;
+    CachedTile best;
+    uint32_t measured = 0;
+    if (hit) {
+      best = *hit;
+    } else {
+      const std::vector<FdTuneResult> r = workspace_measure_tiles(s, w, nq, 3);
+      check_device_flags(s, s.stream);
+      best.tile = r[0].tile;
+      best.ms = r[0].ms;
+      best.default_ms = r[0].ms;
+      for (const FdTuneResult& x : r)
+        if (x.ms < best.ms) {
+          best.tile = x.tile;
+          best.ms = x.ms;
+        }
+      measured = (uint32_t)r.size();
+      append_tune_cache(cache_path, key, best);
+    }
+    fd_set_tile(s.fd, nq, best.tile);
+    if (out) out->push_back(via_scan_tuning{(uint32_t)nq, to_abi(best.tile), best.ms, best.default_ms, measured, 0});
+  }
+  ++s.plan_gen;
+}
+
+}  // namespace via
+
+extern "C" {
+
+via_status via_server_autotune(via_server* s, const uint32_t* batch_sizes, uint64_t count, const char* cache_path,
+                               via_scan_tuning* out) {
+  return guarded([&] {
+    if (!s || !batch_sizes || count == 0 || count > 64)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument or batch list outside 1..64 entries");
+    std::vector<int> sizes;
+    uint32_t bmax = 0;
+    for (uint64_t i = 0; i < count; ++i) {
+      if (batch_sizes[i] == 0 || batch_sizes[i] > 4096)
+        throw ApiError(VIA_ERR_INVALID_ARGUMENT, "batch size outside 1..4096");
+      bmax = std::max(bmax, batch_sizes[i]);
+      sizes.push_back((int)batch_sizes[i]);
+    }
+    std::lock_guard<std::mutex> g(s->mu);
+    if (s->tensor_fd()) ensure_batch(s, bmax);
+    std::vector<via_scan_tuning> res;
+    autotune_scan(*s, *s->ws, sizes, cache_path, &res);
+    if (out)
+      for (size_t i = 0; i < res.size(); ++i) out[i] = res[i];
+  });
+}
+
+via_status via_server_set_scan_tile(via_server* s, uint32_t batch, const via_scan_tile* tile) {
+  return guarded([&] {
+    if (!s || batch == 0 || batch > 4096) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null handle or bad batch size");
+    std::lock_guard<std::mutex> g(s->mu);
+    if (!s->tensor_fd()) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "this server's scan has no tiles (schoolbook ring)");
+    if (!tile) {
+      auto& v = s->fd.tuned;
+      v.erase(std::remove_if(v.begin(), v.end(), [&](const std::pair<int, FdTile>& e) { return e.first == (int)batch; }),
+              v.end());
+    } else {
+      const FdTile t = from_abi(*tile);
+      if (!fd_tile_valid(s->fd, (int)batch, t)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "tile not valid for this batch");
+      fd_set_tile(s->fd, (int)batch, t);
+    }
+    ++s->plan_gen;
+  });
+}
+
+uint64_t via_scan_tile_candidates(via_server* s, uint32_t batch, via_scan_tile* out, uint64_t cap) {
+  if (!s || !s->tensor_fd() || batch == 0 || batch > 4096) return 0;
+  std::vector<FdTile> c;
+  try {
+    c = fd_tile_candidates(s->fd, (int)batch);
+  } catch (...) {
+    return 0;
+  }
+  if (out)
+    for (uint64_t i = 0; i < std::min<uint64_t>(cap, c.size()); ++i) out[i] = to_abi(c[i]);
+  return c.size();
 }
 
 via_status via_server_answer_many_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,

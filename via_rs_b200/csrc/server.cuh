@@ -67,6 +67,7 @@ struct Server {
   std::vector<size_t> repack_off;
   std::unique_ptr<Workspace, WorkspaceDeleter> ws;
   std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
+  int plan_gen = 0;  // bumped when the scan tiles change; captured graphs of older plans are dropped
   bool tensor_fd() const { return fd.planes != nullptr; }
   ~Server();
 };
@@ -101,6 +102,12 @@ void workspace_destroy(Server& s);
 uint8_t* workspace_sel_bytes(Server& s);
 // FirstDim of nq queries: sel_eval [nq][I][2][n1] -> out_eval [nq][J][2][n1] (eval at q2).
 void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, uint8_t* scratch, cudaStream_t st);
+std::vector<FdTuneResult> workspace_measure_tiles(Server& s, Workspace& w, int nq, int reps);
+// The scan autotuner (server.cu): measures (or reads from the cache file) the
+// fastest tile for every batch size on workspace w, records it in s.fd and
+// invalidates captured graphs. The caller holds s.mu.
+void autotune_scan(Server& s, Workspace& w, const std::vector<int>& sizes, const char* cache_path,
+                   std::vector<via_scan_tuning>* out);
 u64* workspace_query(Server& s);
 u64* workspace_answer_mask(Server& s);
 u64* workspace_answer_body(Server& s);

@@ -63,6 +63,7 @@ struct Service {
   Server* s = nullptr;
   via_service_config cfg{};
   bool via_b = false;
+  std::vector<via_scan_tuning> tuning;  // the autotuner's choices at creation
   size_t unit_len = 0;  // u64 per request (one query, or T queries)
   std::vector<Lane> lanes;
   std::mutex mu;
@@ -250,9 +251,18 @@ via_status via_service_create(via_server* s, const via_service_config* cfg, via_
       cap = lo;
     }
     v->lanes.resize(c.lanes);
+    bool tuned = false;
     for (auto& L : v->lanes) {
       L.cap = cap;
       L.ws = workspace_make(*s, cap * T);
+      if (c.autotune && !tuned) {  // on the first lane's workspace, before any graph is captured
+        std::vector<int> sizes;
+        for (int n = 1; n < cap; n *= 2) sizes.push_back(n * T);
+        sizes.push_back(cap * T);
+        std::lock_guard<std::mutex> g(s->mu);
+        autotune_scan(*s, *L.ws, sizes, c.tune_cache, &v->tuning);
+        tuned = true;
+      }
       VIA_CUDA(cudaStreamCreateWithFlags(&L.stream, cudaStreamNonBlocking));
       VIA_CUDA(cudaEventCreateWithFlags(&L.done, cudaEventDisableTiming));
       VIA_CUDA(cudaHostAlloc((void**)&L.h_in, (size_t)cap * v->unit_len * 8, cudaHostAllocDefault));
@@ -274,6 +284,13 @@ via_status via_service_create(via_server* s, const via_service_config* cfg, via_
   } catch (const std::exception& e) {
     return fail(VIA_ERR_CUDA, e.what());
   }
+}
+
+uint64_t via_service_tuning(via_service* v, via_scan_tuning* out, uint64_t cap) {
+  if (!v) return 0;
+  if (out)
+    for (uint64_t i = 0; i < std::min<uint64_t>(cap, v->tuning.size()); ++i) out[i] = v->tuning[i];
+  return v->tuning.size();
 }
 
 via_status via_service_submit(via_service* v, const uint64_t* query, uint64_t n_lwe, uint64_t* ticket) {

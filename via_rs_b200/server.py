@@ -186,6 +186,30 @@ class Server:
         check(_lib.lib().via_first_dim_scan_many_dev(self._h, ctypes.c_void_p(sel_eval_ptr), n_queries,
                                                      ctypes.c_void_p(out_eval_ptr), ctypes.c_void_p(stream)))
 
+    def autotune(self, batch_sizes, cache_path: str | None = None) -> list:
+        """Runs the scan autotuner for these batch sizes (via_server_autotune);
+        returns one dict per size: the tile kept, its time and the default's."""
+        sizes = (ctypes.c_uint32 * len(batch_sizes))(*[int(b) for b in batch_sizes])
+        out = (_lib.ScanTuning * len(batch_sizes))()
+        path = cache_path.encode() if cache_path else None
+        check(_lib.lib().via_server_autotune(self._h, sizes, len(batch_sizes), path, out))
+        return [o.as_dict() for o in out]
+
+    def scan_tile_candidates(self, batch: int) -> list:
+        """The tiles the autotuner tries for `batch` queries (default first)."""
+        L = _lib.lib()
+        n = int(L.via_scan_tile_candidates(self._h, batch, None, 0))
+        out = (_lib.ScanTile * max(1, n))()
+        L.via_scan_tile_candidates(self._h, batch, out, n)
+        return [out[i].as_dict() for i in range(n)]
+
+    def set_scan_tile(self, batch: int, tile: dict | None) -> None:
+        """Forces (or, with None, clears) the scan tile for `batch` queries."""
+        t = None
+        if tile is not None:
+            t = ctypes.byref(_lib.ScanTile(tile.get("n_max", 0), tile.get("stages", 0), tile.get("order", 0), 0))
+        check(_lib.lib().via_server_set_scan_tile(self._h, batch, t))
+
     def close(self) -> None:
         if self._h:
             _lib.lib().via_server_destroy(self._h)

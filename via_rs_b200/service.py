@@ -11,7 +11,8 @@ from .server import Server, check
 
 class ServiceConfig(ctypes.Structure):
     _fields_ = [("lanes", ctypes.c_uint32), ("max_batch", ctypes.c_uint32), ("hbm_budget", ctypes.c_uint64),
-                ("max_pending", ctypes.c_uint32), ("warm", ctypes.c_uint32)]
+                ("max_pending", ctypes.c_uint32), ("warm", ctypes.c_uint32), ("autotune", ctypes.c_uint32),
+                ("tune_cache", ctypes.c_char_p)]
 
 
 class ServiceStats(ctypes.Structure):
@@ -41,6 +42,8 @@ def _bind():
     L.via_server_workspace_bytes.argtypes = [vp, ctypes.c_uint64]
     L.via_service_stats_reset.restype = ctypes.c_int
     L.via_service_stats_reset.argtypes = [vp]
+    L.via_service_tuning.restype = ctypes.c_uint64
+    L.via_service_tuning.argtypes = [vp, ctypes.POINTER(_lib.ScanTuning), ctypes.c_uint64]
     L.via_service_destroy.restype = None
     L.via_service_destroy.argtypes = [vp]
     L._service_bound = True
@@ -58,14 +61,23 @@ class Service:
     poll()/wait() return its (mask, body) answer."""
 
     def __init__(self, server: Server, lanes: int = 2, max_batch: int = 64, hbm_budget: int = 0,
-                 max_pending: int = 0, warm: bool = False):
+                 max_pending: int = 0, warm: bool = False, autotune: bool = False, tune_cache: str | None = None):
         self.server = server
         self.prm = server.prm
         L = _bind()
-        cfg = ServiceConfig(lanes, max_batch, hbm_budget, max_pending, 1 if warm else 0)
+        cfg = ServiceConfig(lanes, max_batch, hbm_budget, max_pending, 1 if warm else 0, 1 if autotune else 0,
+                            tune_cache.encode() if tune_cache else None)
         h = ctypes.c_void_p()
         check(L.via_service_create(server._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
+
+    def tuning(self) -> list:
+        """The scan autotuner's choices made at creation (empty without autotune)."""
+        L = _bind()
+        n = int(L.via_service_tuning(self._h, None, 0))
+        out = (_lib.ScanTuning * max(1, n))()
+        L.via_service_tuning(self._h, out, n)
+        return [out[i].as_dict() for i in range(n)]
 
     def submit(self, query) -> int:
         q = np.ascontiguousarray(query, dtype=np.uint64).reshape(-1)
