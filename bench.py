@@ -61,6 +61,8 @@ def parse():
                     help="requests of the served leg (Poisson arrivals, continuous batching; 0 = skip)")
     ap.add_argument("--via-b", type=int, default=1, help="run the VIA-B leg (T = 8, records of degree 64)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default scan tiles (skip the autotuner)")
+    ap.add_argument("--microbench", type=int, default=1, help="run the kernel micro-benchmark leg (NTT, external "
+                    "product, key switch at n = 2048)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="set up, answer one batch of --batch queries and exit (a short target for ncu)")
     return ap.parse_args()
@@ -255,6 +257,71 @@ def served_leg(args, prm, server, query, rate):
             "scan_tiles": [{"batch": e["batch"], **e["tile"]} for e in tuning]}
 
 
+def microbench_leg(args, peak):
+    """Kernel micro-benchmarks on seeded uniform residues at n = 2048: the NTT of
+    65536 polynomials over both q1 primes, 16384 external products (DMux gadget
+    55879, L = 2 at q1; CMux gadget 81, L = 2 at q2) and 16384 key switches of
+    rotated ciphertexts (conversion-key gadget 18, L = 18 at q1). CUDA events on
+    the launching stream; each call is one whole batch."""
+    import torch
+
+    from via_rs_b200 import prims
+    from via_rs_b200.params import PAPER_Q1, PAPER_Q2
+
+    n = 2048
+    gen = torch.Generator(device="cuda").manual_seed(11)
+    stream = torch.cuda.Stream()
+    sp = stream.cuda_stream
+
+    def rand(q, count):
+        parts = [torch.randint(0, int(qi), (count, 1, n), dtype=torch.int64, device="cuda", generator=gen) for qi in q]
+        return torch.cat(parts, dim=1).contiguous()
+
+    def timed(fn, reps=3):
+        fn()
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(reps):
+            fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    out = {"n": n, "data": "seeded uniform residues (torch Philox seed 11)"}
+    q1 = tuple(PAPER_Q1)
+    r1 = prims.ring(n, q1)
+    polys = 65536
+    x = rand(q1, polys)
+    ntt_bytes = 2 * x.numel() * 8  # read + write of every residue
+    for name, fn in (("ntt_forward", prims.ntt_forward_dev), ("ntt_inverse", prims.ntt_inverse_dev)):
+        ms = timed(lambda: fn(r1, x.data_ptr(), polys, sp))
+        out[name] = {"polys": polys, "primes": 2, "ms": ms, "limb_transforms_s": polys * 2 / ms * 1e3,
+                     "gbs": ntt_bytes / ms / 1e6, "hbm_frac": ntt_bytes / ms / 1e6 / peak}
+    del x
+    pairs = 16384
+    for name, q, base, L in (("external_product_q1", q1, 55879, 2), ("external_product_q2", (PAPER_Q2,), 81, 2)):
+        r = prims.ring(n, q)
+        rg = rand(q, pairs * 2 * L * 2)
+        ct = rand(q, pairs * 2)
+        o = torch.empty_like(ct)
+        ms = timed(lambda: prims.external_product_dev(r, base, L, rg.data_ptr(), ct.data_ptr(), pairs, o.data_ptr(), sp))
+        out[name] = {"pairs": pairs, "base": base, "levels": L, "ms": ms, "per_s": pairs / ms * 1e3}
+        del rg, ct, o
+    L = 18
+    key = rand(q1, L * 2)
+    ct = rand(q1, pairs * 2)
+    shifts = torch.from_numpy(np.random.default_rng(12).integers(0, 2 * n, size=pairs).astype(np.int64)).cuda()
+    o = torch.empty_like(ct)
+    ms = timed(lambda: prims.key_switch_dev(r1, 18, L, key.data_ptr(), ct.data_ptr(), shifts.data_ptr(), pairs,
+                                            o.data_ptr(), sp))
+    out["key_switch_q1"] = {"ciphertexts": pairs, "base": 18, "levels": L, "rotation": "X^k, k uniform in [0, 2n)",
+                            "ms": ms, "per_s": pairs / ms * 1e3}
+    del key, ct, o
+    torch.cuda.empty_cache()
+    return out
+
+
 def via_b_leg(args, prm, rank):
     """answer_batch with T = n2 / n3 = 8 queries per answer over the same number
     of database cells (records of degree 64: 8x the records of the VIA-C leg)."""
@@ -431,6 +498,11 @@ def gpu_arm(args, prm):
     if args.via_b and world == 1:
         via_b = via_b_leg(args, prm, rank)
 
+    # ---- kernel micro-benchmarks (NTT, external product, key switch).
+    micro = None
+    if args.microbench and world == 1:
+        micro = microbench_leg(args, load_peaks()[0])
+
     # ---- roofline of the dominant kernel: the FirstDim scan alone, timed live.
     sel = torch.randint(0, prm.q2, (prm.num_rows * 2 * prm.n1,), dtype=torch.int64, device="cuda")
     out = torch.empty(prm.num_cols * 2 * prm.n1, dtype=torch.int64, device="cuda")
@@ -462,6 +534,7 @@ def gpu_arm(args, prm):
             "batched": batched,
             "served": served,
             "via_b": via_b,
+            "microbench": micro,
             "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols

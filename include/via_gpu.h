@@ -344,6 +344,44 @@ via_status via_server_answer_wire(via_server* s, const uint8_t* wire, uint64_t l
  */
 via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
 
+/*
+ * Primitive operations on caller device buffers, over any NTT-friendly ring
+ * (each prime below 2^50 and = 1 mod 2n; n a power of two in 2..4096). They run
+ * the answer path's kernels on the reference's own operations, for parity
+ * tests and the kernel micro-benchmarks. Layouts are the reference's (limb 0
+ * first; RLWE = mask then body; RGSW = neg_s_m RLev then m RLev, L samples
+ * each, sample 0 paired with the largest gadget entry). Every call is
+ * enqueued on `stream`; the external product and key switch return after
+ * their work has finished (they reuse a per-device scratch buffer).
+ */
+typedef struct via_ring_desc {
+  uint32_t n;     /* degree */
+  uint32_t nl;    /* 1, or 2 for a two-prime RNS modulus q[0] * q[1] */
+  uint64_t q[2];
+} via_ring_desc;
+
+/* In-place negacyclic NTT of `count` ring elements [count][nl][n]: the
+ * reference's cooley_tukey_dit_forward / cooley_tukey_dif_inverse
+ * (algebra/ring/ntt.rs:305-399), with its root (the primitive 2n-th root from
+ * the smallest base, ntt.rs:150-198) and bit-reversed evaluation order, so
+ * the eval form equals the reference's. Outputs are canonical residues. */
+via_status via_ntt_forward_dev(const via_ring_desc* ring, uint64_t* data, uint64_t count, void* stream);
+via_status via_ntt_inverse_dev(const via_ring_desc* ring, uint64_t* data, uint64_t count, void* stream);
+
+/* out[c] = rgsw[c] (x) rlwe[c] (encryption/rgsw.rs:108-121) for `count` pairs,
+ * coefficient form, one gadget (base, levels) for both halves of the RGSW:
+ * rgsw [count][2*levels][2][nl][n], rlwe and out [count][2][nl][n]. */
+via_status via_external_product_dev(const via_ring_desc* ring, uint64_t base, uint32_t levels, const uint64_t* rgsw,
+                                    const uint64_t* rlwe, uint64_t count, uint64_t* out, void* stream);
+
+/* out[c] = key_switch(key, X^shifts[c] * rlwe[c]) (encryption/keyswitch.rs:99-102
+ * after the monomial rotation of algebra/ring/element.rs:328, shift taken mod
+ * 2n): key is one RLev of `levels` samples [levels][2][nl][n] in coefficient
+ * form shared by all; rlwe and out [count][2][nl][n]. */
+via_status via_key_switch_dev(const via_ring_desc* ring, uint64_t base, uint32_t levels, const uint64_t* key,
+                              const uint64_t* rlwe, const uint64_t* shifts, uint64_t count, uint64_t* out,
+                              void* stream);
+
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t via_kernel_launches(void);
 

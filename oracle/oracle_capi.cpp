@@ -3,6 +3,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <thread>
 
 #include "../include/via_gpu.h"
 #include "via_oracle.hpp"
@@ -265,6 +266,80 @@ int vo_server_first_dim(void* sv, const uint64_t* switched, uint64_t* out, int t
       put_poly(d, c.mask);
       put_poly(d, c.body);
     }
+  });
+}
+
+}  // extern "C"
+
+// ---- primitives (include/via_gpu.h via_ntt_*_dev, via_external_product_dev,
+// via_key_switch_dev): the reference operations on flat buffers.
+static Ring prim_ring(uint64_t q0, uint64_t q1, int n) { return q1 ? Ring::rns(n, q0, q1) : Ring::single(n, q0); }
+
+template <class F>
+static void prim_parallel(size_t count, int threads, F f) {
+  threads = std::max(1, std::min<int>(threads, (int)count));
+  std::vector<std::thread> ts;
+  for (int t = 0; t < threads; ++t)
+    ts.emplace_back([&, t] {
+      for (size_t c = t; c < count; c += threads) f(c);
+    });
+  for (auto& th : ts) th.join();
+}
+
+extern "C" {
+
+// algebra/ring/ntt.rs:305-399 on [count][nl][n], in place.
+int vo_ntt(uint64_t q0, uint64_t q1, int n, int inverse, uint64_t* data, size_t count) {
+  return guarded([&] {
+    Ring R = prim_ring(q0, q1, n);
+    if (!R.eval_is_ntt()) throw OracleError(ERR_INVALID, "ring is not NTT-friendly");
+    for (size_t c = 0; c < count; ++c) {
+      u64* p = data + c * R.size();
+      Poly a(p, p + R.size());
+      Poly r = inverse ? R.from_eval(a) : R.to_eval(a);
+      std::memcpy(p, r.data(), r.size() * 8);
+    }
+  });
+}
+
+// encryption/rgsw.rs:108-121 for `count` pairs, one gadget for both halves.
+int vo_external_product(uint64_t q0, uint64_t q1, int n, uint64_t base, int L, const uint64_t* rgsw,
+                        const uint64_t* rlwe, size_t count, uint64_t* out, int threads) {
+  return guarded([&] {
+    Ring R = prim_ring(q0, q1, n);
+    const size_t per = R.size();
+    prim_parallel(count, threads, [&](size_t c) {
+      const u64* src = rgsw + c * 2 * L * 2 * per;
+      Rgsw g;
+      g.neg_s_m = get_rlev(src, R, L);
+      g.m = get_rlev(src, R, L);
+      const u64* cs = rlwe + c * 2 * per;
+      Rlwe ct{get_poly(cs, per), get_poly(cs, per)};
+      Rlwe r = external_product(R, rgsw_to_eval(R, g), ct, base, base);
+      u64* d = out + c * 2 * per;
+      put_poly(d, r.mask);
+      put_poly(d, r.body);
+    });
+  });
+}
+
+// key_switch (encryption/keyswitch.rs:99-102) of X^k * ct (element.rs:328).
+int vo_key_switch(uint64_t q0, uint64_t q1, int n, uint64_t base, int L, const uint64_t* key, const uint64_t* rlwe,
+                  const uint64_t* shifts, size_t count, uint64_t* out, int threads) {
+  return guarded([&] {
+    Ring R = prim_ring(q0, q1, n);
+    const size_t per = R.size();
+    const u64* ks = key;
+    const RlevEval K = rlev_to_eval(R, get_rlev(ks, R, L));
+    prim_parallel(count, threads, [&](size_t c) {
+      const u64* cs = rlwe + c * 2 * per;
+      Rlwe ct{get_poly(cs, per), get_poly(cs, per)};
+      Rlwe rot{R.mul_x_pow(ct.mask, shifts[c]), R.mul_x_pow(ct.body, shifts[c])};
+      Rlwe r = key_switch(R, K, rot, base);
+      u64* d = out + c * 2 * per;
+      put_poly(d, r.mask);
+      put_poly(d, r.body);
+    });
   });
 }
 

@@ -51,6 +51,11 @@ def lib() -> ctypes.CDLL:
         L.vo_server_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, ctypes.c_int, _u64p, ctypes.c_int]
         L.vo_stage_times.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.vo_shake256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
+        L.vo_ntt.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _u64p, ctypes.c_size_t]
+        L.vo_external_product.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
+                                          ctypes.c_int, _u64p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
+        L.vo_key_switch.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64, ctypes.c_int,
+                                    _u64p, _u64p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
         _lib = L
     return _lib
 
@@ -90,6 +95,43 @@ def kat(layer: str, scenario: str, name: str, cap: int = 4096) -> np.ndarray:
     if n < 0:
         raise OracleError(-n, f"{layer}/{scenario}/{name}: " + lib().vo_last_error().decode())
     return out[:n].copy()
+
+
+def _u64c(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def ntt(q: tuple, n: int, data, inverse: bool = False) -> np.ndarray:
+    """The reference's negacyclic NTT (ntt.rs:305-399) of [count][nl][n] residues
+    over the primes q = (q0,) or (q0, q1); returns a new array."""
+    out = _u64c(data).copy()
+    q1 = q[1] if len(q) > 1 else 0
+    _check(lib().vo_ntt(q[0], q1, n, 1 if inverse else 0, _ptr(out), out.size // (len(q) * n)))
+    return out
+
+
+def external_product(q: tuple, n: int, base: int, L: int, rgsw, rlwe, threads: int = 0) -> np.ndarray:
+    """RGSW (x) RLWE (rgsw.rs:108-121) per pair: rgsw [c][2L][2][nl][n], rlwe [c][2][nl][n]."""
+    rg, ct = _u64c(rgsw), _u64c(rlwe)
+    nl = len(q)
+    count = ct.size // (2 * nl * n)
+    out = np.zeros(count * 2 * nl * n, dtype=np.uint64)
+    q1 = q[1] if nl > 1 else 0
+    _check(lib().vo_external_product(q[0], q1, n, base, L, _ptr(rg), _ptr(ct), count, _ptr(out),
+                                     threads or os.cpu_count() or 1))
+    return out
+
+
+def key_switch(q: tuple, n: int, base: int, L: int, key, rlwe, shifts, threads: int = 0) -> np.ndarray:
+    """key_switch(key, X^k ct) (keyswitch.rs:99-102, element.rs:328) per ciphertext."""
+    k, ct, sh = _u64c(key), _u64c(rlwe), _u64c(shifts)
+    nl = len(q)
+    count = ct.size // (2 * nl * n)
+    out = np.zeros(count * 2 * nl * n, dtype=np.uint64)
+    q1 = q[1] if nl > 1 else 0
+    _check(lib().vo_key_switch(q[0], q1, n, base, L, _ptr(k), _ptr(ct), _ptr(sh), count, _ptr(out),
+                               threads or os.cpu_count() or 1))
+    return out
 
 
 class Client:

@@ -21,6 +21,11 @@ class ViaPublicKeys(ctypes.Structure):
     _fields_ = [("cascade_key", _u64p), ("conv_key", _u64p), ("rsk", _u64p)]
 
 
+class RingDesc(ctypes.Structure):
+    """via_ring_desc: degree, limb count and primes of a ring."""
+    _fields_ = [("n", ctypes.c_uint32), ("nl", ctypes.c_uint32), ("q", ctypes.c_uint64 * 2)]
+
+
 class ScanTile(ctypes.Structure):
     """via_scan_tile: one FirstDim scan tile choice."""
     _fields_ = [("n_max", ctypes.c_uint32), ("stages", ctypes.c_uint32), ("order", ctypes.c_uint32),
@@ -108,6 +113,16 @@ def lib() -> ctypes.CDLL:
     L.via_scan_tile_candidates.restype = ctypes.c_uint64
     L.via_scan_tile_candidates.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ScanTile),
                                            ctypes.c_uint64]
+    R = ctypes.POINTER(RingDesc)
+    vp = ctypes.c_void_p
+    for name in ("via_ntt_forward_dev", "via_ntt_inverse_dev"):
+        f = getattr(L, name)
+        f.restype = ctypes.c_int
+        f.argtypes = [R, vp, ctypes.c_uint64, vp]
+    L.via_external_product_dev.restype = ctypes.c_int
+    L.via_external_product_dev.argtypes = [R, ctypes.c_uint64, ctypes.c_uint32, vp, vp, ctypes.c_uint64, vp, vp]
+    L.via_key_switch_dev.restype = ctypes.c_int
+    L.via_key_switch_dev.argtypes = [R, ctypes.c_uint64, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint64, vp, vp]
     L.via_kernel_launches.restype = ctypes.c_uint64
     L.via_kernel_launches.argtypes = []
     _lib = L

@@ -1199,4 +1199,77 @@ void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_bo
   answer_batch_device(s, *s.ws, d_queries, 1, d_mask, d_body, st);
 }
 
+
+// ===========================================================================
+// Standalone primitives (the reference's own kernel-level operations, on
+// caller buffers; coefficient form in and out).
+// ===========================================================================
+
+// External products ext[c] = rgsw[c] (x) ct[c] (crates/via-primitives/src/
+// encryption/rgsw.rs:108-121): every RGSW is transformed once per call (the
+// reference re-transforms its samples per call too, rlev.rs:211-219), then the
+// mask and body digits meet the neg_s_m and m samples.
+//   rgsw [count][2L][2][nl][n], cts/out [count][2][nl][n].
+// Scratch: rgsw_eval (count * 2L * 2 * nl * n), digits (count * 2L * nl * n).
+void prim_external_products(const DevRing& R, const Gadget& g, const u64* rgsw, const u64* cts, long count, u64* out,
+                            u64* rgsw_eval, u64* digits, cudaStream_t st) {
+  const long per = (long)R.nl * R.n;
+  VIA_CUDA(cudaMemcpyAsync(rgsw_eval, rgsw, (size_t)count * 2 * g.L * 2 * per * 8, cudaMemcpyDeviceToDevice, st));
+  to_eval(R, rgsw_eval, R.n, count * 2 * g.L * 2 * R.nl, st);
+  external_products(R, g, KeySel{rgsw_eval, 1, count, 0}, cts, count, digits, out, true, st);
+}
+
+// X^k a (negacyclic) of mask and body, split into masks [count][nl][n] and
+// bodies [count][nl][n] (element.rs:328, ops.rs:147-180).
+__global__ void k_rotate_split(const u64* __restrict__ cts, const u64* __restrict__ shifts, long count, int n, int nl,
+                               DevRing R, u64* __restrict__ masks, u64* __restrict__ bodies) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long per = (long)nl * n;
+  if (gid >= count * 2 * per) return;
+  const long c = gid / (2 * per);
+  const int part = (int)((gid / per) % 2);
+  const int l = (int)((gid % per) / n), i = (int)(gid % n);
+  const u64 k = shifts[c] % (u64)(2 * n);
+  const u64 v = cts[gid];
+  const u64 pos = (u64)i + k;  // < 3n
+  const int dst = (int)(pos % (u64)n);
+  const bool neg = ((pos / (u64)n) & 1) != 0;
+  const u64 q = R.m[l].q;
+  u64* o = (part == 0 ? masks : bodies) + c * per + (long)l * n;
+  o[dst] = neg && v ? q - v : v;
+}
+
+// out = (-prod.mask, body - prod.body) (keyswitch.rs:99-102).
+__global__ void k_key_switch_finish(const u64* __restrict__ prod, const u64* __restrict__ bodies, long count, int n,
+                                    int nl, DevRing R, u64* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long per = (long)nl * n;
+  if (gid >= count * per) return;
+  const long c = gid / per;
+  const long r = gid % per;
+  const int l = (int)(r / n);
+  const u64 q = R.m[l].q;
+  const u64 pm = prod[(2 * c) * per + r], pb = prod[(2 * c + 1) * per + r];
+  out[(2 * c) * per + r] = pm ? q - pm : 0;
+  out[(2 * c + 1) * per + r] = submod(bodies[c * per + r], pb, q);
+}
+
+// Key switches of rotated ciphertexts: out[c] = key_switch(K, X^{shift[c]} ct[c]).
+//   key: RLev of L samples [L][2][nl][n] (coefficient form), shared by all.
+// Scratch: key_eval (L * 2 * nl * n), masks/bodies (count * nl * n each),
+// digits (count * L * nl * n), prod (count * 2 * nl * n).
+void prim_key_switches(const DevRing& R, const Gadget& g, const u64* key, const u64* cts, const u64* shifts, long count,
+                       u64* out, u64* key_eval, u64* masks, u64* bodies, u64* digits, u64* prod, cudaStream_t st) {
+  const int n = R.n;
+  const long per = (long)R.nl * n;
+  VIA_CUDA(cudaMemcpyAsync(key_eval, key, (size_t)g.L * 2 * per * 8, cudaMemcpyDeviceToDevice, st));
+  to_eval(R, key_eval, n, (long)g.L * 2 * R.nl, st);
+  k_rotate_split<<<blocks(count * 2 * per), 256, 0, st>>>(cts, shifts, count, n, R.nl, R, masks, bodies);
+  VIA_LAUNCHED();
+  gadget_product(R, g, masks, n, 1, 1, count, keys_shared(key_eval), prod, digits, st);
+  from_eval(R, prod, n, count * 2 * R.nl, st);
+  k_key_switch_finish<<<blocks(count * per), 256, 0, st>>>(prod, bodies, count, n, R.nl, R, out);
+  VIA_LAUNCHED();
+}
+
 }  // namespace via

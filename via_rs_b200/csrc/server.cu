@@ -110,7 +110,7 @@ u64 cascade_key_len(const via_params& p) {
 u64 conv_key_len(const via_params& p) { return (u64)p.l_ck * 2 * (p.q1_1 ? 2 : 1) * p.n1; }
 u64 rsk_len(const via_params& p) { return (u64)(p.n1 / p.n2) * p.l_rsk * 2 * p.n2; }
 
-static u64 h_inv(u64 a, u64 m) {
+u64 h_inv(u64 a, u64 m) {
   i128 t = 0, nt = 1, r = m, nr = a % m;
   while (nr) {
     i128 qq = r / nr, tmp = t - qq * nt;

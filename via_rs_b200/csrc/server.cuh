@@ -81,6 +81,7 @@ u64 cascade_key_len(const via_params& p);
 u64 conv_key_len(const via_params& p);
 u64 rsk_len(const via_params& p);
 int ilog2(u64 v);
+u64 h_inv(u64 a, u64 m);  // a^-1 mod m, 0 if not invertible
 
 // Pipeline entry points (pipeline.cu).
 constexpr int STOP_AFTER_CROT = -1;  // answer_device_stages: leave the CRot outputs in the workspace
