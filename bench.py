@@ -60,6 +60,8 @@ def parse():
     ap.add_argument("--served", type=int, default=384,
                     help="requests of the served leg (Poisson arrivals, continuous batching; 0 = skip)")
     ap.add_argument("--via-b", type=int, default=1, help="run the VIA-B leg (T = 8, records of degree 64)")
+    ap.add_argument("--mixed", type=int, default=24, help="requests in the mixed VIA-C / VIA-B served leg (0 = skip)")
+    ap.add_argument("--mixed-rate", type=float, default=2.0, help="arrival rate (requests/s) of the mixed leg")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default scan tiles (skip the autotuner)")
     ap.add_argument("--microbench", type=int, default=1, help="run the kernel micro-benchmark leg (NTT, external "
                     "product, key switch at n = 2048)")
@@ -322,6 +324,77 @@ def microbench_leg(args, peak):
     return out
 
 
+def mixed_leg(args, prm, server, rate):
+    """A seeded Poisson stream of VIA-C queries and VIA-B requests of 1..256
+    indices (log-uniform), padded to T = 8 (records of degree 64) or T = 256
+    (degree 2), served from the one prepared database through three views with a
+    continuous-batching service each. Returns throughput, padding and p50/p99;
+    one request of each kind is re-answered alone and compared."""
+    import torch
+
+    from via_rs_b200.mixed import MixedService, poisson_mix, via_b_route
+
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free * 0.6)
+    mix = MixedService(server, lanes=2, hbm_budget=budget, shares={"c": 0.35, 8: 0.15, 256: 0.5},
+                       autotune=not args.no_autotune)
+    rng = np.random.default_rng(21)
+    qmin = min(prm.q1)
+
+    def queries(route):
+        pv = mix.params(route)
+        count = 1 if route == "c" else route
+        return rng.integers(0, qmin, size=count * pv.n_lwe * pv.lwe_len, dtype=np.uint64)
+
+    plan = []
+    for gap, kind, m in poisson_mix(args.mixed, rate, seed=22):
+        route = "c" if kind == "c" else via_b_route(m)
+        plan.append((gap, route, m, queries(route)))
+    try:
+        for route in ("c", 8, 256):  # one warm request per route
+            mix.wait(mix.submit(route, queries(route)))
+        mix.reset_stats()
+        handles = []
+        t0 = time.perf_counter()
+        due = t0
+        for gap, route, m, q in plan:
+            due += gap
+            while time.perf_counter() < due:
+                time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+            handles.append(mix.submit(route, q))
+        answers = [mix.wait(h) for h in handles]
+        wall = time.perf_counter() - t0
+        lat = mix.latencies()
+        exact = True
+        for route in ("c", 8, 256):
+            k = next((i for i, p in enumerate(plan) if p[1] == route), None)
+            if k is None:
+                continue
+            srv = mix.servers[route]
+            alone = srv.answer(plan[k][3]) if route == "c" else srv.answer_batch(plan[k][3].reshape(route, -1))
+            exact = exact and np.array_equal(alone[0], answers[k][0]) and np.array_equal(alone[1], answers[k][1])
+    finally:
+        mix.close()
+    n_c = sum(1 for p in plan if p[1] == "c")
+    b = [p for p in plan if p[1] != "c"]
+    records = n_c + sum(p[2] for p in b)
+    slots = sum(p[1] for p in b)
+    all_lat = np.concatenate([v for v in lat.values() if len(v)])
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+
+    return {"requests": len(plan), "via_c": n_c, "via_b_t8": sum(1 for p in b if p[1] == 8),
+            "via_b_t256": sum(1 for p in b if p[1] == 256), "offered_rate_hz": rate,
+            "requests_s": len(plan) / wall, "records_s": records / wall,
+            "answers_s": len(plan) / wall, "padding_frac": (slots - sum(p[2] for p in b)) / max(1, slots),
+            "p50_ms": pct(all_lat, 50), "p99_ms": pct(all_lat, 99),
+            "p50_ms_by_route": {str(k): pct(v, 50) for k, v in lat.items()},
+            "p99_ms_by_route": {str(k): pct(v, 99) for k, v in lat.items()},
+            "hbm_budget_bytes": budget, "sampled_bit_exact": bool(exact),
+            "arrivals": "seeded Poisson (numpy PCG64 seed 22), half VIA-C, VIA-B sizes log-uniform in 1..256"}
+
+
 def via_b_leg(args, prm, rank):
     """answer_batch with T = n2 / n3 = 8 queries per answer over the same number
     of database cells (records of degree 64: 8x the records of the VIA-C leg)."""
@@ -493,6 +566,11 @@ def gpu_arm(args, prm):
     if args.served > 0:
         served = served_leg(args, prm, server, query, rate=0.85 * (batched["answers_s"] if batched else value))
 
+    # ---- mixed VIA-C / VIA-B stream over views of the same database.
+    mixed = None
+    if args.mixed > 0 and world == 1:
+        mixed = mixed_leg(args, prm, server, args.mixed_rate)
+
     # ---- VIA-B: T = 8 records of degree 64 per answer on a second (1 GiB) server.
     via_b = None
     if args.via_b and world == 1:
@@ -535,6 +613,7 @@ def gpu_arm(args, prm):
             "served": served,
             "via_b": via_b,
             "microbench": micro,
+            "mixed": mixed,
             "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols

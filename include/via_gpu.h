@@ -121,6 +121,20 @@ via_status via_server_setup(const via_params* params, const via_public_keys* key
                             uint64_t n_records, via_record_format format, via_server** out);
 
 /*
+ * A second server handle over the prepared database of `base` (no copy) with
+ * another record degree: n_rec = n2 for VIA-C, or a VIA-B n3 dividing n2. The
+ * database is a grid of I x J cells of n1 plaintext coefficients; a server
+ * reads it as records of degree n_rec, record k*I*J + i*J + j being
+ * coefficients d*c + k (c < n_rec, d = n1 / n_rec) of cell (i, j), which is how
+ * setup_db (setup_db.rs:39-75) places records of that degree. So one copy of a
+ * database in HBM serves VIA-C queries and VIA-B batches of any T side by side.
+ * `keys` may be the base's or another client's. The cells stay alive while
+ * any handle over them does; destroy handles in any order. The reference
+ * builds one Server per record degree, each with its own PreparedDb.
+ */
+via_status via_server_view(via_server* base, uint32_t n_rec, const via_public_keys* keys, via_server** out);
+
+/*
  * Server::answer (answer.rs:534-554): steps 1-7 on the device for one query.
  * out_mask: n2 residues mod q3; out_body: n2 residues mod q4. Host buffers.
  */
@@ -250,7 +264,10 @@ via_status via_debug_stage(via_server* s, const uint64_t* query, uint64_t n_lwe,
  */
 via_status via_server_answer_batch(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
                                    uint64_t* out_mask, uint64_t* out_body);
-/* The same on device buffers, enqueued on `stream`. */
+/* The same on device buffers, enqueued on `stream` (`queries` is read in place,
+ * so it must stay valid until the stream reaches the end of this work). Both
+ * entry points run batches of more than 64 queries (T = 256) through their
+ * prefix in chunks of 64, each chunk sharing one database scan. */
 via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, uint64_t n_queries, uint64_t n_lwe,
                                        uint64_t* out_mask, uint64_t* out_body, void* stream);
 
@@ -263,8 +280,11 @@ via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, u
  * capacity is the largest batch whose workspace fits hbm_budget / lanes, capped
  * by max_batch; requests beyond it wait for a free lane. A VIA-C server serves
  * single queries; a VIA-B server (n_rec < n2) serves groups of T = n2 / n_rec
- * queries, one answer per group. Results do not depend on how requests are
+ * queries, one answer per group; a group larger than a lane's workspace runs
+ * alone, its prefix in chunks. Results do not depend on how requests are
  * batched. Every wait is bounded; no host thread blocks inside the driver.
+ * Services over views of one database (via_server_view) serve VIA-C queries
+ * and VIA-B batches of several T from a single copy of the database.
  */
 typedef struct via_service via_service;
 
@@ -305,6 +325,10 @@ via_status via_service_wait(via_service* v, uint64_t ticket, uint64_t* out_mask,
 via_status via_service_stats_get(via_service* v, via_service_stats* out);
 /* Zeroes the counters and latency record (requests in flight still complete). */
 via_status via_service_stats_reset(via_service* v);
+/* Submit-to-completion latencies (milliseconds) of the requests completed since
+ * creation or the last stats reset, in completion order: returns their number
+ * and writes up to `cap` of them to `out` (may be NULL). */
+uint64_t via_service_latencies(via_service* v, double* out, uint64_t cap);
 /* The autotuner's choices made at creation (cfg.autotune): returns their
  * number and writes up to `cap` entries to `out` (may be NULL). */
 uint64_t via_service_tuning(via_service* v, via_scan_tuning* out, uint64_t cap);

@@ -68,6 +68,9 @@ def lib() -> ctypes.CDLL:
     L.via_server_setup.restype = ctypes.c_int
     L.via_server_setup.argtypes = [P, ctypes.POINTER(ViaPublicKeys), ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
                                    ctypes.POINTER(ctypes.c_void_p)]
+    L.via_server_view.restype = ctypes.c_int
+    L.via_server_view.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ViaPublicKeys),
+                                  ctypes.POINTER(ctypes.c_void_p)]
     L.via_server_answer.restype = ctypes.c_int
     L.via_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_uint64, _u64p, _u64p]
     L.via_server_destroy.restype = None

@@ -444,7 +444,7 @@ void first_dim_queries(Server& s, const u64* sel_eval, u64* out_eval, int nq, ui
     return;
   }
   for (int q = 0; q < nq; ++q)
-    first_dim_schoolbook(s.db.p, sel_eval + (size_t)q * p.num_rows * 2 * p.n1, out_eval + (size_t)q * p.num_cols * 2 * p.n1,
+    first_dim_schoolbook(s.db->p, sel_eval + (size_t)q * p.num_rows * 2 * p.n1, out_eval + (size_t)q * p.num_cols * 2 * p.n1,
                          (int)p.num_rows, (int)p.num_cols, (int)p.n1, s.r2.m[0], st);
 }
 
@@ -1109,6 +1109,7 @@ void derive_repack_keys(Server& s) {
 struct RepackWs {
   int T = 0;
   DevBuf la_m, la_b, lb_m, lb_b, emb_m, emb_b, digits, P, bsum, packed;
+  DevBuf crot_all;  // CRot outputs of a batch run in chunks [T * groups][2][n1]
   Gadget g;
 };
 
@@ -1131,6 +1132,7 @@ static RepackWs& repack_ws(Server& s, Workspace& w) {
     r->P.alloc(pairs * 4 * n1);
     r->bsum.alloc(pairs * n1);
     r->g = make_gadget(p.ck_base, (int)p.l_ck, s.r2.Q());
+    if (T > w.bmax) r->crot_all.alloc(T * 2 * n1);  // one batch runs in chunks of bmax queries
     w.repack = std::move(r);
   }
   return *w.repack;
@@ -1187,11 +1189,31 @@ void answer_batch_device(Server& s, Workspace& w, const u64* d_queries, int grou
   const int n1 = s.prm.n1;
   if (T < 2) throw CudaError(100, "answer_batch: the server was set up for VIA-C (n_rec = n2)");
   if (!s.repack_eval.p) throw CudaError(100, "answer_batch: no repack keys");
-  answer_device_stages(s, w, d_queries, T * groups, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
   RepackWs& r = repack_ws(s, w);
+  const int total = T * groups;
+  const u64* crot = w.cr_ct.p;
+  if (total <= w.bmax) {
+    answer_device_stages(s, w, d_queries, total, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
+  } else {
+    // More queries than the workspace holds: the prefix runs in chunks of bmax
+    // queries (each chunk shares one database scan) and the CRot outputs are
+    // gathered for the repack. Memory stays that of a bmax-query workspace.
+    if (r.crot_all.n < (size_t)total * 2 * n1) {
+      VIA_CUDA(cudaStreamSynchronize(st));
+      r.crot_all.alloc((size_t)total * 2 * n1);
+    }
+    const size_t qlen = (size_t)query_lwes(s.prm) * lwe_len(s.prm);
+    for (int q0 = 0; q0 < total; q0 += w.bmax) {
+      const int nc = std::min(w.bmax, total - q0);
+      answer_device_stages(s, w, d_queries + (size_t)q0 * qlen, nc, nullptr, nullptr, st, STOP_AFTER_CROT, nullptr);
+      VIA_CUDA(cudaMemcpyAsync(r.crot_all.p + (size_t)q0 * 2 * n1, w.cr_ct.p, (size_t)nc * 2 * n1 * 8,
+                               cudaMemcpyDeviceToDevice, st));
+    }
+    crot = r.crot_all.p;
+  }
   if (!r.packed.p || r.packed.n < (size_t)groups * 2 * n1) r.packed.alloc((size_t)groups * 2 * n1);
   for (int g = 0; g < groups; ++g)
-    repack(s, w, w.cr_ct.p + (size_t)g * T * 2 * n1, r.packed.p + (size_t)g * 2 * n1, st);
+    repack(s, w, crot + (size_t)g * T * 2 * n1, r.packed.p + (size_t)g * 2 * n1, st);
   resp_comp(s, w, r.packed.p, groups, d_mask, d_body, st);
 }
 

@@ -199,6 +199,20 @@ static void transform_keys(Server& s) {
     ntt_forward(s.rsk_eval.p, p.n2, 1, (long)(p.n1 / p.n2) * p.l_rsk * 2, s.r3.t[0], s.r3.t[1], s.stream);
 }
 
+static void load_keys(Server& s, const via_public_keys* keys) {
+  if (!keys) return;
+  const via_params& p = s.prm;
+  if (!keys->cascade_key || !keys->conv_key || !keys->rsk) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null key buffer");
+  s.cascade_eval.alloc(cascade_key_len(p));
+  s.conv_eval.alloc(conv_key_len(p));
+  s.rsk_eval.alloc(rsk_len(p));
+  VIA_CUDA(cudaMemcpyAsync(s.cascade_eval.p, keys->cascade_key, s.cascade_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+  VIA_CUDA(cudaMemcpyAsync(s.conv_eval.p, keys->conv_key, s.conv_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+  VIA_CUDA(cudaMemcpyAsync(s.rsk_eval.p, keys->rsk, s.rsk_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
+  derive_repack_keys(s);  // VIA-B: from the coefficient-form cascade key, before it is transformed
+  transform_keys(s);
+}
+
 static void setup(Server& s, const via_params& p, const via_public_keys* keys, const void* records, u64 n_records,
                   via_record_format fmt) {
   validate_params(p);
@@ -235,16 +249,18 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     s.fd.m = s.r2.m[0];
     VIA_CUDA(cudaDeviceGetAttribute(&s.fd.grid, cudaDevAttrMultiProcessorCount, s.device));
     s.fd.smem_max = fd_prepare_device();
-    s.planes.alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1) / 8);
-    VIA_CUDA(cudaMemsetAsync(s.planes.p, 0, s.planes.n * 8, s.stream));
+    s.planes = std::make_shared<DevBuf>();
+    s.planes->alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1) / 8);
+    VIA_CUDA(cudaMemsetAsync(s.planes->p, 0, s.planes->n * 8, s.stream));
     s.fd_err.alloc(1);
     VIA_CUDA(cudaMemsetAsync(s.fd_err.p, 0, 8, s.stream));
     s.fd.err = reinterpret_cast<int*>(s.fd_err.p);
     cells.alloc(rows_per_pass * J * p.n1);
   } else {
-    s.db.alloc(I * J * p.n1);
+    s.db = std::make_shared<DevBuf>();
+    s.db->alloc(I * J * p.n1);
   }
-  u64* cell_buf = tensor ? cells.p : s.db.p;
+  u64* cell_buf = tensor ? cells.p : s.db->p;
   void* stage = nullptr;
   if (n_records) VIA_CUDA(cudaMalloc(&stage, (size_t)std::min<u64>(rows_per_pass * J, n_records) * rec_bytes));
   try {
@@ -266,8 +282,8 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
       }
       if (s.r2.ntt) ntt_forward(cell_buf, p.n1, 1, (long)(rows * J), s.r2.t[0], s.r2.t[0], s.stream);
       if (tensor) {
-        s.fd.planes = reinterpret_cast<const uint8_t*>(s.planes.p);
-        fd_rows_to_planes(cell_buf, (int)i0, s.fd, reinterpret_cast<uint8_t*>(s.planes.p), s.stream);
+        s.fd.planes = reinterpret_cast<const uint8_t*>(s.planes->p);
+        fd_rows_to_planes(cell_buf, (int)i0, s.fd, reinterpret_cast<uint8_t*>(s.planes->p), s.stream);
       }
     }
   } catch (...) {
@@ -278,18 +294,38 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
   VIA_CUDA(cudaStreamSynchronize(s.stream));
   cells.free();
 
-  // Keys.
-  if (keys) {
-    if (!keys->cascade_key || !keys->conv_key || !keys->rsk) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null key buffer");
-    s.cascade_eval.alloc(cascade_key_len(p));
-    s.conv_eval.alloc(conv_key_len(p));
-    s.rsk_eval.alloc(rsk_len(p));
-    VIA_CUDA(cudaMemcpyAsync(s.cascade_eval.p, keys->cascade_key, s.cascade_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
-    VIA_CUDA(cudaMemcpyAsync(s.conv_eval.p, keys->conv_key, s.conv_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
-    VIA_CUDA(cudaMemcpyAsync(s.rsk_eval.p, keys->rsk, s.rsk_eval.n * 8, cudaMemcpyHostToDevice, s.stream));
-    derive_repack_keys(s);  // VIA-B: from the coefficient-form cascade key, before it is transformed
-    transform_keys(s);
+  load_keys(s, keys);
+  workspace_create(s, 1);
+  VIA_CUDA(cudaStreamSynchronize(s.stream));
+}
+
+// A second handle over the prepared database of `base` with record degree
+// n_rec: the cells (and their planes) are shared, not copied. Only n_rec may
+// differ from the base's parameters; the view's record r = k*I*J + i*J + j is
+// coefficients d*c + k (d = n1 / n_rec) of cell (i, j), as setup_db lays out
+// records of that degree (setup_db.rs:39-75).
+static void setup_view(Server& s, const Server& base, uint32_t n_rec, const via_public_keys* keys) {
+  via_params p = base.prm;
+  p.n_rec = n_rec;
+  validate_params(p);
+  s.prm = p;
+  VIA_CUDA(cudaGetDevice(&s.device));
+  if (s.device != base.device) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "a view must be made on its database's device");
+  VIA_CUDA(cudaStreamCreateWithFlags(&s.stream, cudaStreamNonBlocking));
+  s.r1 = make_ring(s, p.n1, p.q1_0, p.q1_1);
+  s.r2 = make_ring(s, p.n1, p.q2, 0);
+  s.r3n1 = make_ring(s, p.n1, p.q3, 0);
+  s.r3 = make_ring(s, p.n2, p.q3, 0);
+  s.r4 = make_ring(s, p.n2, p.q4, 0);
+  s.db = base.db;
+  s.planes = base.planes;
+  s.fd = base.fd;  // geometry, device limits and tuned tiles
+  if (s.planes) {
+    s.fd_err.alloc(1);
+    VIA_CUDA(cudaMemsetAsync(s.fd_err.p, 0, 8, s.stream));
+    s.fd.err = reinterpret_cast<int*>(s.fd_err.p);
   }
+  load_keys(s, keys);
   workspace_create(s, 1);
   VIA_CUDA(cudaStreamSynchronize(s.stream));
 }
@@ -315,6 +351,16 @@ via_status via_server_setup(const via_params* params, const via_public_keys* key
     *out = nullptr;
     std::unique_ptr<via_server> s(new via_server());
     setup(*s, *params, keys, records, n_records, format);
+    *out = s.release();
+  });
+}
+
+via_status via_server_view(via_server* base, uint32_t n_rec, const via_public_keys* keys, via_server** out) {
+  return guarded([&] {
+    if (!base || !out) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    *out = nullptr;
+    std::unique_ptr<via_server> s(new via_server());
+    setup_view(*s, *base, n_rec, keys);
     *out = s.release();
   });
 }
@@ -670,11 +716,10 @@ via_status via_server_answer_batch_dev(via_server* s, const uint64_t* queries, u
     check_batch(s, n_queries, n_lwe);
     const via_params& p = s->prm;
     cudaStream_t st = (cudaStream_t)stream;
+    (void)p;
     std::lock_guard<std::mutex> g(s->mu);
-    ensure_batch(s, n_queries);
-    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
-                             cudaMemcpyDeviceToDevice, st));
-    answer_batch_device(*s, workspace_query(*s), out_mask, out_body, st);
+    ensure_batch(s, std::min<u64>(n_queries, VIA_B_CHUNK));
+    answer_batch_device(*s, queries, out_mask, out_body, st);
   });
 }
 
@@ -685,10 +730,16 @@ via_status via_server_answer_batch(via_server* s, const uint64_t* queries, uint6
     check_batch(s, n_queries, n_lwe);
     const via_params& p = s->prm;
     std::lock_guard<std::mutex> g(s->mu);
-    ensure_batch(s, n_queries);
-    VIA_CUDA(cudaMemcpyAsync(workspace_query(*s), queries, n_queries * n_lwe * lwe_len(p) * 8,
-                             cudaMemcpyHostToDevice, s->stream));
-    answer_batch_device(*s, workspace_query(*s), workspace_answer_mask(*s), workspace_answer_body(*s), s->stream);
+    ensure_batch(s, std::min<u64>(n_queries, VIA_B_CHUNK));
+    const size_t bytes = n_queries * n_lwe * lwe_len(p) * 8;
+    DevBuf big;  // a batch larger than the workspace is uploaded whole and answered in chunks
+    u64* dq = workspace_query(*s);
+    if (n_queries > (u64)workspace_batch(*s)) {
+      big.alloc(bytes / 8);
+      dq = big.p;
+    }
+    VIA_CUDA(cudaMemcpyAsync(dq, queries, bytes, cudaMemcpyHostToDevice, s->stream));
+    answer_batch_device(*s, dq, workspace_answer_mask(*s), workspace_answer_body(*s), s->stream);
     VIA_CUDA(cudaMemcpyAsync(out_mask, workspace_answer_mask(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaMemcpyAsync(out_body, workspace_answer_body(*s), p.n2 * 8, cudaMemcpyDeviceToHost, s->stream));
     VIA_CUDA(cudaStreamSynchronize(s->stream));

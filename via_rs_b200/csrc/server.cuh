@@ -53,8 +53,9 @@ struct Server {
   // Prepared database. NTT-friendly q2: byte planes for the tensor-core scan
   // (fd_tc.cuh layout) in `planes`, described by `fd`. Otherwise (schoolbook
   // rings): [I][J][n1] u64 residues in `db`.
-  DevBuf db;
-  DevBuf planes;
+  // Shared with the views of this database (via_server_view).
+  std::shared_ptr<DevBuf> db;
+  std::shared_ptr<DevBuf> planes;
   FdPlan fd;
   DevBuf fd_err;  // one device word the scan sets when a bounded wait runs out
   // Eval-form keys (crates/via-server/src/prepared_keys.rs:69-79).
@@ -87,6 +88,9 @@ u64 h_inv(u64 a, u64 m);  // a^-1 mod m, 0 if not invertible
 constexpr int STOP_AFTER_CROT = -1;  // answer_device_stages: leave the CRot outputs in the workspace
 // VIA-B batch size T = n2 / n_rec (the record-fit boundary); 1 for VIA-C servers.
 inline int via_b_batch(const via_params& p) { return (int)(p.n2 / p.n_rec); }
+// Queries per workspace pass of the synchronous VIA-B entry points: larger
+// batches run their prefix in chunks of this many queries.
+constexpr int VIA_B_CHUNK = 64;
 void derive_repack_keys(Server& s);
 void answer_batch_device(Server& s, const u64* d_queries, u64* d_mask, u64* d_body, cudaStream_t st);
 void workspace_create(Server& s, int bmax);

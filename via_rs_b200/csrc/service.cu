@@ -52,6 +52,7 @@ struct Lane {
   u64* h_mask = nullptr;  // pinned: cap answers
   u64* h_body = nullptr;
   int* h_err = nullptr;  // pinned copy of the scan's error word
+  std::unique_ptr<DevBuf> d_in;  // VIA-B requests larger than the workspace: their queries, answered in chunks
   int cap = 0;
   bool busy = false;
   std::vector<Request*> batch;
@@ -117,9 +118,10 @@ void Service::launch(Lane& L) {
     L.batch.push_back(r);
   }
   try {
-    VIA_CUDA(cudaMemcpyAsync(ws_query(*L.ws), L.h_in, (size_t)n * unit_len * 8, cudaMemcpyHostToDevice, L.stream));
+    u64* d_in = L.d_in ? L.d_in->p : ws_query(*L.ws);
+    VIA_CUDA(cudaMemcpyAsync(d_in, L.h_in, (size_t)n * unit_len * 8, cudaMemcpyHostToDevice, L.stream));
     if (via_b)
-      answer_batch_device(*s, *L.ws, ws_query(*L.ws), n, ws_answer_mask(*L.ws), ws_answer_body(*L.ws), L.stream);
+      answer_batch_device(*s, *L.ws, d_in, n, ws_answer_mask(*L.ws), ws_answer_body(*L.ws), L.stream);
     else
       answer_graph(*s, *L.ws, n, L.stream);
     VIA_CUDA(cudaMemcpyAsync(L.h_mask, ws_answer_mask(*L.ws), (size_t)n * p.n2 * 8, cudaMemcpyDeviceToHost, L.stream));
@@ -233,32 +235,42 @@ via_status via_service_create(via_server* s, const via_service_config* cfg, via_
     const int T = v->via_b ? via_b_batch(p) : 1;
     v->unit_len = (size_t)T * query_lwes(p) * lwe_len(p);
     VIA_CUDA(cudaSetDevice(s->device));
-    // Admission: the largest per-lane batch (in requests) whose workspace fits
-    // this lane's share of the HBM budget.
-    int cap = (int)c.max_batch;
+    // Admission: each lane's workspace holds `qcap` queries, the most whose
+    // device memory fits the lane's share of the HBM budget (up to max_batch
+    // requests). A lane batch is cap = qcap / T requests; a VIA-B request
+    // larger than the workspace (T > qcap) runs alone, its prefix in chunks of
+    // qcap queries, with its T queries held in a separate device buffer.
+    const size_t qbytes = (size_t)query_lwes(p) * lwe_len(p) * 8;
+    auto lane_bytes = [&](int q) { return workspace_bytes(*s, q) + (q < T ? (size_t)T * qbytes : 0); };
+    int qcap = (int)c.max_batch * T;
+    if (v->via_b && !c.hbm_budget && T > VIA_B_CHUNK) qcap = VIA_B_CHUNK;
     if (c.hbm_budget) {
       const size_t share = c.hbm_budget / c.lanes;
-      if (workspace_bytes(*s, T) > share)
+      if (lane_bytes(1) > share)
         return fail(VIA_ERR_OUT_OF_MEMORY, "via_service_create: hbm_budget / lanes = " + std::to_string(share) +
-                                               " bytes is below one request's workspace (" +
-                                               std::to_string(workspace_bytes(*s, T)) + " bytes)");
-      int lo = 1, hi = cap;  // workspace bytes grow with the batch: largest fitting batch
+                                               " bytes is below one query's workspace (" +
+                                               std::to_string(lane_bytes(1)) + " bytes)");
+      int lo = 1, hi = qcap;  // device bytes grow with the batch: largest fitting query count
       while (lo < hi) {
         const int mid = (lo + hi + 1) / 2;
-        if (workspace_bytes(*s, mid * T) <= share) lo = mid;
+        if (lane_bytes(mid) <= share) lo = mid;
         else hi = mid - 1;
       }
-      cap = lo;
+      qcap = lo;
     }
+    const int cap = std::max(1, qcap / T);
+    if (qcap >= T) qcap = cap * T;
     v->lanes.resize(c.lanes);
     bool tuned = false;
     for (auto& L : v->lanes) {
       L.cap = cap;
-      L.ws = workspace_make(*s, cap * T);
+      L.ws = workspace_make(*s, qcap);
+      if (qcap < T) L.d_in.reset(new DevBuf((size_t)T * qbytes / 8));
       if (c.autotune && !tuned) {  // on the first lane's workspace, before any graph is captured
         std::vector<int> sizes;
-        for (int n = 1; n < cap; n *= 2) sizes.push_back(n * T);
-        sizes.push_back(cap * T);
+        const int top = std::min(qcap, cap * T);
+        for (int n = T; n < top; n *= 2) sizes.push_back(n);
+        sizes.push_back(top);
         std::lock_guard<std::mutex> g(s->mu);
         autotune_scan(*s, *L.ws, sizes, c.tune_cache, &v->tuning);
         tuned = true;
@@ -284,6 +296,14 @@ via_status via_service_create(via_server* s, const via_service_config* cfg, via_
   } catch (const std::exception& e) {
     return fail(VIA_ERR_CUDA, e.what());
   }
+}
+
+uint64_t via_service_latencies(via_service* v, double* out, uint64_t cap) {
+  if (!v) return 0;
+  std::lock_guard<std::mutex> lk(v->mu);
+  if (out)
+    for (uint64_t i = 0; i < std::min<uint64_t>(cap, v->latencies.size()); ++i) out[i] = v->latencies[i];
+  return v->latencies.size();
 }
 
 uint64_t via_service_tuning(via_service* v, via_scan_tuning* out, uint64_t cap) {

@@ -112,6 +112,19 @@ class Server:
         s._keys = keys
         return s
 
+    def view(self, n_rec: int, keys: PublicKeys | None = None) -> "Server":
+        """A handle over this server's prepared database (shared, not copied) that
+        reads it as records of degree n_rec (via_server_view): VIA-C (n2) or a
+        VIA-B n3. `keys` defaults to this server's keys."""
+        keys = keys if keys is not None else self._keys
+        prm = self.prm.with_dims(self.prm.num_rows, self.prm.num_cols, n_rec)
+        k = _lib.ViaPublicKeys(_ptr(keys.cascade_key), _ptr(keys.conv_key), _ptr(keys.rsk))
+        h = ctypes.c_void_p()
+        check(_lib.lib().via_server_view(self._h, n_rec, ctypes.byref(k), ctypes.byref(h)))
+        s = Server(h, prm)
+        s._keys = keys
+        return s
+
     def answer(self, query):
         """Server::answer: returns (mask mod q3, body mod q4), n2 residues each."""
         q = _u64(query)

@@ -42,6 +42,8 @@ def _bind():
     L.via_server_workspace_bytes.argtypes = [vp, ctypes.c_uint64]
     L.via_service_stats_reset.restype = ctypes.c_int
     L.via_service_stats_reset.argtypes = [vp]
+    L.via_service_latencies.restype = ctypes.c_uint64
+    L.via_service_latencies.argtypes = [vp, ctypes.POINTER(ctypes.c_double), ctypes.c_uint64]
     L.via_service_tuning.restype = ctypes.c_uint64
     L.via_service_tuning.argtypes = [vp, ctypes.POINTER(_lib.ScanTuning), ctypes.c_uint64]
     L.via_service_destroy.restype = None
@@ -70,6 +72,15 @@ class Service:
         h = ctypes.c_void_p()
         check(L.via_service_create(server._h, ctypes.byref(cfg), ctypes.byref(h)))
         self._h = h
+
+    def latencies(self) -> np.ndarray:
+        """Submit-to-completion latencies (ms) of the requests completed since
+        creation or the last reset, in completion order."""
+        L = _bind()
+        n = int(L.via_service_latencies(self._h, None, 0))
+        out = np.zeros(max(1, n), dtype=np.float64)
+        n = int(L.via_service_latencies(self._h, out.ctypes.data_as(ctypes.POINTER(ctypes.c_double)), n))
+        return out[:n]
 
     def tuning(self) -> list:
         """The scan autotuner's choices made at creation (empty without autotune)."""
