@@ -365,6 +365,7 @@ def mixed_leg(args, prm, server, rate):
         answers = [mix.wait(h) for h in handles]
         wall = time.perf_counter() - t0
         lat = mix.latencies()
+        mix.close_services()  # frees the lanes before the views answer alone
         exact = True
         for route in ("c", 8, 256):
             k = next((i for i, p in enumerate(plan) if p[1] == route), None)

@@ -66,13 +66,18 @@ class MixedService:
         for s in self.services.values():
             s.reset_stats()
 
-    def close(self) -> None:
+    def close_services(self) -> None:
+        """Stops the services and frees their lanes; the views stay usable."""
         for s in self.services.values():
             s.close()
+        self.services = {}
+
+    def close(self) -> None:
+        self.close_services()
         for k, srv in self.servers.items():
             if k != "c":
                 srv.close()
-        self.services = {}
+        self.servers = {"c": self.base}
 
 
 def poisson_mix(n: int, rate_hz: float, seed: int, via_c_fraction: float = 0.5, max_indices: int = 256):
