@@ -259,7 +259,7 @@ def served_leg(args, prm, server, query, rate):
             "scan_tiles": [{"batch": e["batch"], **e["tile"]} for e in tuning]}
 
 
-def microbench_leg(args, peak):
+def microbench_leg(args, prm, peak):
     """Kernel micro-benchmarks on seeded uniform residues at n = 2048: the NTT of
     65536 polynomials over both q1 primes, 16384 external products (DMux gadget
     55879, L = 2 at q1; CMux gadget 81, L = 2 at q2) and 16384 key switches of
@@ -321,7 +321,40 @@ def microbench_leg(args, peak):
                             "ms": ms, "per_s": pairs / ms * 1e3}
     del key, ct, o
     torch.cuda.empty_cache()
+    out["client"] = client_microbench(prm)
     return out
+
+
+def client_microbench(prm):
+    """Device client at the bench's preset and grid: 64 queries generated per call
+    (one seeded PRG stream each) and 256 answers recovered per call."""
+    from via_rs_b200.client import Client
+
+    rng = np.random.default_rng(13)
+    ternary = rng.integers(-1, 2, size=prm.nl * prm.n1)
+    sk1 = np.concatenate([np.where(ternary[l * prm.n1:(l + 1) * prm.n1] < 0, q + ternary[l * prm.n1:(l + 1) * prm.n1],
+                                   ternary[l * prm.n1:(l + 1) * prm.n1]).astype(np.uint64)
+                          for l, q in enumerate(prm.q1)])
+    s2 = rng.integers(-1, 2, size=prm.n2)
+    sk2 = np.where(s2 < 0, prm.q3 + s2, s2).astype(np.uint64)
+    c = Client(prm, sk1, sk2)
+    n = 64
+    idx = rng.integers(prm.capacity, size=n)
+    seeds = [b"bench-%04d" % k for k in range(n)]
+    c.queries(idx[:2], seeds[:2])
+    t0 = time.perf_counter()
+    c.queries(idx, seeds)
+    tq = time.perf_counter() - t0
+    masks = rng.integers(0, prm.q3, size=(256, prm.n2), dtype=np.uint64)
+    bodies = rng.integers(0, prm.q4, size=(256, prm.n2), dtype=np.uint64)
+    c.recover_many(masks[:2], bodies[:2])
+    t0 = time.perf_counter()
+    c.recover_many(masks, bodies)
+    tr = time.perf_counter() - t0
+    c.close()
+    return {"queries": n, "query_ms": tq * 1e3, "queries_s": n / tq, "query_bytes": int(prm.n_lwe * prm.lwe_len * 8),
+            "recovers": 256, "recover_ms": tr * 1e3, "recovers_s": 256 / tr,
+            "timing": "host wall clock around the synchronous call (host buffers, copies included)"}
 
 
 def mixed_leg(args, prm, server, rate):
@@ -580,7 +613,7 @@ def gpu_arm(args, prm):
     # ---- kernel micro-benchmarks (NTT, external product, key switch).
     micro = None
     if args.microbench and world == 1:
-        micro = microbench_leg(args, load_peaks()[0])
+        micro = microbench_leg(args, prm, load_peaks()[0])
 
     # ---- roofline of the dominant kernel: the FirstDim scan alone, timed live.
     sel = torch.randint(0, prm.q2, (prm.num_rows * 2 * prm.n1,), dtype=torch.int64, device="cuda")

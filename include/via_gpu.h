@@ -406,6 +406,37 @@ via_status via_key_switch_dev(const via_ring_desc* ring, uint64_t base, uint32_t
                               const uint64_t* rlwe, const uint64_t* shifts, uint64_t count, uint64_t* out,
                               void* stream);
 
+/*
+ * The client side on the device (crates/via-client/src), for load generation at
+ * serving rates and for clients holding many queries. The client's secret keys
+ * come from its keygen (cli/client.rs:89-180): sk1 is nl * n1 residues at q1
+ * (limb 0 first), sk2 is n2 residues at q3. err_kind 0 samples ternary errors,
+ * 1 bounded-uniform errors in [-err_bound, err_bound] (distribution.rs:88-118).
+ */
+typedef struct via_client via_client;
+via_status via_client_create(const via_params* params, const uint64_t* sk1, const uint64_t* sk2, uint32_t err_kind,
+                             uint32_t err_bound, via_client** out);
+void via_client_destroy(via_client* c);
+
+/* Client::query (cli/query.rs:75-130) for `count` indices: query k is drawn from
+ * Shake256Prg(seeds + k * seed_len) (seed_len in 1..64 bytes), exactly as the
+ * reference client would draw it from that PRG. Each query has via_query_len
+ * LWEs (d = n1 / n_rec selects the CRot bits) in the via_server_answer layout;
+ * `out` (host) receives count queries back to back. The PRG blocks are computed
+ * in parallel, one warp walks each query's rejection-sampled stream, and the
+ * inner products run one CTA per LWE. VIA_ERR_INDEX_OUT_OF_RANGE for an index
+ * >= d * I * J. */
+via_status via_client_queries(via_client* c, const uint64_t* indices, uint64_t count, const uint8_t* seeds,
+                              uint32_t seed_len, uint64_t* out);
+/* The same into device memory, enqueued on `stream`; returns after the work is done. */
+via_status via_client_queries_dev(via_client* c, const uint64_t* indices, uint64_t count, const uint8_t* seeds,
+                                  uint32_t seed_len, uint64_t* out, void* stream);
+/* Client::recover for `count` answers (decrypt_asymmetric, encryption/rlwe.rs:187-240):
+ * masks and bodies [count][n2] (host), out [count][n2] plaintext coefficients mod p.
+ * VIA-B answers hold record t at coefficients t + T * k (recover_batch, cli/batch.rs:35-58). */
+via_status via_client_recover(via_client* c, const uint64_t* masks, const uint64_t* bodies, uint64_t count,
+                              uint64_t* out);
+
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t via_kernel_launches(void);
 

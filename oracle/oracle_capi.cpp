@@ -179,6 +179,14 @@ int vo_client_recover(void* c, const uint64_t* mask, const uint64_t* body, uint6
   });
 }
 
+// The client's secret keys (S1 at q1, nl * n1 residues; S2 at q3, n2 residues),
+// for the device client's parity tests.
+void vo_client_secret(void* c, uint64_t* sk1, uint64_t* sk2) {
+  const Client* cl = (const Client*)c;
+  std::memcpy(sk1, cl->sk1.data(), cl->sk1.size() * 8);
+  std::memcpy(sk2, cl->sk2.data(), cl->sk2.size() * 8);
+}
+
 void vo_client_free(void* c) { delete (Client*)c; }
 
 // Server::setup (srv/answer.rs:486-528). Records: n_rec u64 coefficients each.

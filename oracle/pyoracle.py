@@ -40,6 +40,7 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_size_t, _u64p]
         L.vo_client_recover.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p]
         L.vo_client_free.argtypes = [ctypes.c_void_p]
+        L.vo_client_secret.argtypes = [ctypes.c_void_p, _u64p, _u64p]
         L.vo_server_setup.restype = ctypes.c_void_p
         L.vo_server_setup.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p, _u64p, ctypes.c_size_t, ctypes.c_int]
         L.vo_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, _u64p, ctypes.c_int]
@@ -160,6 +161,14 @@ class Client:
     def batch_query(self, indices, seed: bytes) -> np.ndarray:
         """Client::batch_query (cli/client.rs:256-300): one query per index at d3 = n1 / n_rec."""
         return np.stack([self.query(int(i), seed + b"-%d" % k) for k, i in enumerate(indices)])
+
+    def secret_keys(self):
+        """(S1 [nl * n1] at q1, S2 [n2] at q3), for the device client's tests."""
+        prm = self.prm
+        sk1 = np.zeros(prm.nl * prm.n1, dtype=np.uint64)
+        sk2 = np.zeros(prm.n2, dtype=np.uint64)
+        lib().vo_client_secret(self._h, _ptr(sk1), _ptr(sk2))
+        return sk1, sk2
 
     def recover_batch(self, mask: np.ndarray, body: np.ndarray) -> list:
         """Client::recover_batch (cli/client.rs:316-333, cli/batch.rs:35-58): record t is
