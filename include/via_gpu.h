@@ -437,6 +437,14 @@ via_status via_client_queries_dev(via_client* c, const uint64_t* indices, uint64
 via_status via_client_recover(via_client* c, const uint64_t* masks, const uint64_t* bodies, uint64_t count,
                               uint64_t* out);
 
+/* The gadget decomposition the kernels run (gadget.rs:115-190: centred lift,
+ * round(|c| B^L / Q), balanced base-B digits LSB-first), evaluated on the host
+ * for `count` coefficients given as residues (nl per coefficient; q1 = 0 for a
+ * single modulus). out: count * levels digits. No device work: it checks the
+ * exact scaling against the reference on machines without a GPU. */
+via_status via_gadget_digits_host(uint64_t q0, uint64_t q1, uint64_t base, uint32_t levels, const uint64_t* coeffs,
+                                  uint64_t count, int64_t* out);
+
 /* Number of kernels this library has launched since it was loaded. */
 uint64_t via_kernel_launches(void);
 

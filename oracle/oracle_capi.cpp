@@ -296,6 +296,25 @@ static void prim_parallel(size_t count, int threads, F f) {
 
 extern "C" {
 
+// gadget_scale_into + gadget_extract_lsb_into (encryption/gadget.rs:115-190) per
+// coefficient (nl residues each): count * L digits, LSB first.
+int vo_gadget_digits(uint64_t q0, uint64_t q1, uint64_t base, int L, const uint64_t* coeffs, size_t count,
+                     int64_t* out) {
+  return guarded([&] {
+    Ring R = q1 ? Ring::rns(1, q0, q1) : Ring::single(1, q0);
+    std::vector<i128> scratch;
+    std::vector<i64> dig;
+    for (size_t i = 0; i < count; ++i) {
+      Poly x(coeffs + i * R.nl, coeffs + (i + 1) * R.nl);
+      gadget_scale_into(R, x, base, L, scratch);
+      for (int k = 0; k < L; ++k) {
+        gadget_extract_lsb_into(base, scratch, dig);
+        out[i * L + k] = dig[0];
+      }
+    }
+  });
+}
+
 // algebra/ring/ntt.rs:305-399 on [count][nl][n], in place.
 int vo_ntt(uint64_t q0, uint64_t q1, int n, int inverse, uint64_t* data, size_t count) {
   return guarded([&] {

@@ -52,6 +52,8 @@ def lib() -> ctypes.CDLL:
         L.vo_server_debug_stage.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, ctypes.c_int, _u64p, ctypes.c_int]
         L.vo_stage_times.argtypes = [ctypes.POINTER(ctypes.c_double)]
         L.vo_shake256.argtypes = [ctypes.c_char_p, ctypes.c_size_t, ctypes.c_char_p, ctypes.c_size_t]
+        L.vo_gadget_digits.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, _u64p,
+                                       ctypes.c_size_t, ctypes.POINTER(ctypes.c_int64)]
         L.vo_ntt.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_int, _u64p, ctypes.c_size_t]
         L.vo_external_product.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_int, ctypes.c_uint64,
                                           ctypes.c_int, _u64p, _u64p, ctypes.c_size_t, _u64p, ctypes.c_int]
@@ -100,6 +102,16 @@ def kat(layer: str, scenario: str, name: str, cap: int = 4096) -> np.ndarray:
 
 def _u64c(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.uint64)
+
+
+def gadget_digits(q: tuple, base: int, L: int, coeffs) -> np.ndarray:
+    """Balanced gadget digits (gadget.rs:115-190) of coefficients [count][nl]: [count][L]."""
+    c = _u64c(coeffs)
+    count = c.size // len(q)
+    out = np.zeros(count * L, dtype=np.int64)
+    q1 = q[1] if len(q) > 1 else 0
+    _check(lib().vo_gadget_digits(q[0], q1, base, L, _ptr(c), count, out.ctypes.data_as(ctypes.POINTER(ctypes.c_int64))))
+    return out.reshape(count, L)
 
 
 def ntt(q: tuple, n: int, data, inverse: bool = False) -> np.ndarray:

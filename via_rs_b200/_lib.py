@@ -126,6 +126,10 @@ def lib() -> ctypes.CDLL:
     L.via_external_product_dev.argtypes = [R, ctypes.c_uint64, ctypes.c_uint32, vp, vp, ctypes.c_uint64, vp, vp]
     L.via_key_switch_dev.restype = ctypes.c_int
     L.via_key_switch_dev.argtypes = [R, ctypes.c_uint64, ctypes.c_uint32, vp, vp, vp, ctypes.c_uint64, vp, vp]
+    L.via_gadget_digits_host.restype = ctypes.c_int
+    L.via_gadget_digits_host.argtypes = [ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint64, ctypes.c_uint32,
+                                         ctypes.POINTER(ctypes.c_uint64), ctypes.c_uint64,
+                                         ctypes.POINTER(ctypes.c_int64)]
     L.via_kernel_launches.restype = ctypes.c_uint64
     L.via_kernel_launches.argtypes = []
     _lib = L

@@ -122,8 +122,10 @@ __host__ __device__ __forceinline__ void mac128(Acc128& acc, u64 a, u64 b) {
 
 // Signed residue lift of a small integer into [0, q).
 __host__ __device__ __forceinline__ u64 lift_i64(i64 v, const DevMod& m) {
-  if (v >= 0) return reduce64((u64)v, m);
-  u64 r = reduce64((u64)(-v), m);
+  if (v >= 0) return (u64)v < m.q ? (u64)v : reduce64((u64)v, m);
+  const u64 a = (u64)(-v);
+  if (a < m.q) return m.q - a;  // a > 0
+  u64 r = reduce64(a, m);
   return r == 0 ? 0 : m.q - r;
 }
 

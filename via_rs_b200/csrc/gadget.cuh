@@ -60,6 +60,70 @@ __host__ __device__ __forceinline__ u128 crt2(u64 a0, u64 a1, const DevRing& R) 
 }
 
 // ---------------------------------------------------------------------------
+// Division by an invariant 64-bit divisor (Moller and Granlund, "Improved
+// division by invariant integers", IEEE Trans. Computers 60(2), 2011,
+// Algorithm 4): the divisor is normalized (top bit set) and its reciprocal
+// v = floor((2^128 - 1) / d) - 2^64 precomputed, so a 128-by-64 division is two
+// multiplications and two fix-ups.
+// ---------------------------------------------------------------------------
+struct Div64 {
+  u64 d = 1;   // divisor
+  u64 dn = 0;  // d << s
+  u64 v = 0;   // reciprocal of dn
+  int s = 0;   // leading zeros of d
+};
+
+inline Div64 make_div64(u64 d) {
+  Div64 r;
+  r.d = d;
+  r.s = __builtin_clzll(d);
+  r.dn = d << r.s;
+  r.v = (u64)((~(u128)0) / r.dn - ((u128)1 << 64));
+  return r;
+}
+
+// (u1 * 2^64 + u0) / dn for u1 < dn: quotient, remainder in r.
+__host__ __device__ __forceinline__ u64 div_2by1(u64 u1, u64 u0, const Div64& D, u64& r) {
+  u64 q0 = D.v * u1;
+  u64 q1 = mulhi(D.v, u1);
+  const u64 s0 = q0 + u0;
+  q1 += u1 + (s0 < q0 ? 1 : 0);
+  q0 = s0;
+  q1 += 1;
+  u64 rr = u0 - q1 * D.dn;
+  if (rr > q0) {
+    q1 -= 1;
+    rr += D.dn;
+  }
+  if (rr >= D.dn) {
+    q1 += 1;
+    rr -= D.dn;
+  }
+  r = rr;
+  return q1;
+}
+
+// floor(n / d) and n mod d for a 128-bit n and a 64-bit divisor.
+__host__ __device__ __forceinline__ u128 div128by64(u128 n, const Div64& D, u64& rem) {
+  const u64 hi = (u64)(n >> 64), lo = (u64)n;
+  const int s = D.s;
+  const u64 n2 = s ? hi >> (64 - s) : 0;
+  const u64 n1 = s ? (hi << s) | (lo >> (64 - s)) : hi;
+  const u64 n0 = lo << s;
+  u64 r1, r0;
+  const u64 qh = div_2by1(n2, n1, D, r1);
+  const u64 ql = div_2by1(r1, n0, D, r0);
+  rem = r0 >> s;
+  return ((u128)qh << 64) | ql;
+}
+
+// u128 x u64 -> u128 (the product must fit).
+__host__ __device__ __forceinline__ u128 mul128x64(u128 a, u64 b) {
+  const u64 lo = (u64)a;
+  return ((u128)mulhi(lo, b) << 64 | (u128)(lo * b)) + ((u128)((u64)(a >> 64) * b) << 64);
+}
+
+// ---------------------------------------------------------------------------
 // Gadget decomposition (prim/encryption/gadget.rs:115-190).
 // ---------------------------------------------------------------------------
 struct Gadget {
@@ -73,9 +137,21 @@ struct Gadget {
   u64 half_base;
   u64 magic;      // floor(2^64 / B) for the 64-bit digit divisions
   bool small;     // Q * (S + 1) < 2^53: one limb, and the scaling is exact in doubles
+  // Exact integer scaling round(|c| S / Q):
+  //  mode 0: one modulus Q < 2^64 with Q * S < 2^127: num = |c| S + floor(Q/2)
+  //          fits 128 bits, one 128-by-64 division by Q;
+  //  mode 1: Q = q0 * q1 (RNS) with S * max(q0, q1) < 2^127: c = a0 + q0 t, and
+  //          floor(num / Q) = floor((floor((a0 S + floor(Q/2)) / q0) + t S) / q1),
+  //          two 128-by-64 divisions (exact: the remainder of the first division
+  //          is below q0 and cannot carry into the second quotient);
+  //  mode 2: otherwise, the double-precision estimate with exact fix-ups.
+  int mode;
+  Div64 dq, dq1;  // mode 0: Q; mode 1: q0 and q1
+  u64 q0, q1;     // mode 1 limbs
+  Div64 dbc;      // B^c, for the two-chunk split when S >= 2^64
 };
 
-inline Gadget make_gadget(u64 base, int L, u128 Q) {
+inline Gadget make_gadget(u64 base, int L, u128 Q, u64 q0 = 0, u64 q1 = 0) {
   Gadget g{};
   g.base = base;
   g.L = L;
@@ -106,7 +182,30 @@ inline Gadget make_gadget(u64 base, int L, u128 Q) {
   g.half_base = base / 2;
   g.magic = (u64)(((u128)1 << 64) / base);
   g.small = Q < ((u128)1 << 53) && S < ((u128)1 << 53) && Q * (S + 1) < ((u128)1 << 53);
+  // Exact integer scaling mode (see the struct). (long double) products only
+  // decide the mode; the arithmetic itself is exact.
+  const long double lS = (long double)(u64)(S >> 64) * 18446744073709551616.0L + (long double)(u64)S;
+  const long double lQ = (long double)(u64)(Q >> 64) * 18446744073709551616.0L + (long double)(u64)Q;
+  const long double two127 = 170141183460469231731687303715884105728.0L;
+  if ((Q >> 64) == 0 && lQ * (lS + 1) < two127) {
+    g.mode = 0;
+    g.dq = make_div64((u64)Q);
+  } else if (q0 && q1 && (u128)q0 * q1 == Q && lS * (long double)(q0 > q1 ? q0 : q1) * 2 < two127) {
+    g.mode = 1;
+    g.q0 = q0;
+    g.q1 = q1;
+    g.dq = make_div64(q0);
+    g.dq1 = make_div64(q1);
+  } else {
+    g.mode = 2;
+  }
+  if (c < L) g.dbc = make_div64((u64)Bc);
   return g;
+}
+
+// The gadget of a ring: Q and (for a two-prime RNS ring) its limbs.
+inline Gadget make_gadget(u64 base, int L, const DevRing& R) {
+  return R.nl == 2 ? make_gadget(base, L, R.Q(), R.m[0].q, R.m[1].q) : make_gadget(base, L, R.Q());
 }
 
 // u / B and u % B for u < 2^63 via a reciprocal and a fix-up.
@@ -137,30 +236,37 @@ __host__ __device__ __forceinline__ u64 digits64(u64 u, int cnt, const Gadget& g
   return u;
 }
 
+// floor(n / d) for a 64-bit n.
+__host__ __device__ __forceinline__ u64 div64by64(u64 n, const Div64& D, u64& rem) {
+  const int s = D.s;
+  const u64 n1 = s ? n >> (64 - s) : 0, n0 = n << s;
+  u64 r;
+  const u64 q = div_2by1(n1, n0, D, r);
+  rem = r >> s;
+  return q;
+}
+
 // The scaled value of one coefficient reduced mod B^L into [0, B^L): the
-// centred lift c (v <= Q/2 ? v : v - Q), then round(|c| B^L / Q) with c's sign
-// (gadget.rs:115-151). The balanced digits (gadget.rs:168-190) depend only on
+// centred lift c (v <= Q/2 ? v : v - Q), then round(|c| B^L / Q) =
+// floor((|c| B^L + floor(Q/2)) / Q) with c's sign (gadget.rs:115-151,
+// wide.rs:145-153). The balanced digits (gadget.rs:168-190) depend only on
 // this value mod B^L.
-// The scaled value for a `small` gadget (one limb, Q (S + 1) < 2^53): mag * S +
-// floor(Q/2) is an exact double, so one division and a +-1 fix give the exact
-// quotient. The result is below S < 2^53 and is the single digit chunk.
+// A `small` gadget (one limb, Q (S + 1) < 2^53) has a 64-bit numerator and a
+// result below S < 2^53, the single digit chunk.
 __host__ __device__ __forceinline__ u64 gadget_scaled_small(u64 a0, const Gadget& g) {
   const u64 Q = (u64)g.Q, hq = (u64)g.halfQ, S = (u64)g.S;
   const bool neg = a0 > hq;
   const u64 mag = neg ? Q - a0 : a0;
-  const u64 num = mag * S + hq;
-  u64 qe = (u64)((double)num / g.dQ);
-  for (int it = 0; it < 2 && qe * Q > num; ++it) --qe;
-  for (int it = 0; it < 2 && num - qe * Q >= Q; ++it) ++qe;
+  u64 r;
+  const u64 qe = div64by64(mag * S + hq, g.dq, r);
   return (neg && qe != 0) ? S - qe : qe;
 }
 
-__host__ __device__ __forceinline__ u128 gadget_scaled(u64 a0, u64 a1, const DevRing& R, const Gadget& g) {
-  if (g.small) return (u128)gadget_scaled_small(a0, g);
-  u128 v = R.nl == 2 ? crt2(a0, a1, R) : (u128)a0;
+// Mode 2 (large single-limb moduli): a double-precision quotient estimate and
+// exact integer fix-ups.
+__host__ __device__ __forceinline__ u128 gadget_scaled_fp(u128 v, const Gadget& g) {
   bool neg = v > g.halfQ;
   u128 mag = neg ? g.Q - v : v;
-  // floor((mag * S + floor(Q/2)) / Q), exact (wide.rs:145-153).
   u128 qe = double_to_u128(u128_to_double(mag) * g.dS_over_Q);
   i128 r = (i128)(mag * g.S + g.halfQ - qe * g.Q);
   i128 qc = (i128)(i64)floor(i128_to_double(r) / g.dQ);
@@ -177,6 +283,36 @@ __host__ __device__ __forceinline__ u128 gadget_scaled(u64 a0, u64 a1, const Dev
   return (neg && qe != 0) ? g.S - qe : qe;
 }
 
+__host__ __device__ __forceinline__ u128 gadget_scaled(u64 a0, u64 a1, const DevRing& R, const Gadget& g) {
+  if (g.small) return (u128)gadget_scaled_small(a0, g);
+  if (g.mode == 1) {
+    // c = a0 + q0 t with the CRT digit t = (a1 - a0) q0^-1 mod q1.
+    const DevMod& m1 = R.m[1];
+    const u64 t = mul_shoup(submod(a1, reduce64(a0, m1), m1.q), R.q0inv_mod_q1, R.q0inv_shoup, m1.q);
+    const u128 c = (u128)a0 + (u128)g.q0 * t;
+    const bool neg = c > g.halfQ;
+    // |c| = a + q0 u in the same mixed radix.
+    u64 a = a0, u = t;
+    if (neg) {
+      a = a0 ? g.q0 - a0 : 0;
+      u = a0 ? g.q1 - 1 - t : g.q1 - t;
+    }
+    u64 rem;
+    const u128 x1 = div128by64(mul128x64(g.S, a) + g.halfQ, g.dq, rem);
+    const u128 qe = div128by64(x1 + mul128x64(g.S, u), g.dq1, rem);
+    return (neg && qe != 0) ? g.S - qe : qe;
+  }
+  const u128 v = R.nl == 2 ? crt2(a0, a1, R) : (u128)a0;
+  if (g.mode == 0) {
+    const bool neg = v > g.halfQ;
+    const u64 mag = (u64)(neg ? g.Q - v : v);
+    u64 rem;
+    const u128 qe = div128by64(mul128x64(g.S, mag) + g.halfQ, g.dq, rem);
+    return (neg && qe != 0) ? g.S - qe : qe;
+  }
+  return gadget_scaled_fp(v, g);
+}
+
 // Splits the scaled value into the two 64-bit chunks the digit loop consumes:
 // lo < B^c holds digits 0..c-1, hi holds digits c..L-1 (plus lo's carry).
 __host__ __device__ __forceinline__ void gadget_chunks(u128 u, const Gadget& g, u64& lo, u64& hi) {
@@ -184,9 +320,9 @@ __host__ __device__ __forceinline__ void gadget_chunks(u128 u, const Gadget& g, 
     lo = (u64)u;
     hi = 0;
   } else {
-    u128 uh = div_exact(u, (u128)g.Bc, g.dBc);
-    lo = (u64)(u - uh * (u128)g.Bc);
-    hi = (u64)uh;
+    u64 rem;
+    hi = (u64)div128by64(u, g.dbc, rem);
+    lo = rem;
   }
 }
 

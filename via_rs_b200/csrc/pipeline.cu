@@ -497,7 +497,7 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
     A(w->sel_bytes, (bytes + 7) / 8);
   }
   A(w->fd_out, B * J * 2 * n1);
-  const bool fused = cmux_fused_ok(s.r2, make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q()));
+  const bool fused = cmux_fused_ok(s.r2, make_gadget(p.b_cmux, (int)p.l_query, s.r2));
   A(w->cm_diff, fused ? 0 : B * std::max(1L, J / 2) * 2 * n1);
   A(w->cm_digits, fused ? 0 : B * std::max(1L, J / 2) * 2 * L * n1);
   A(w->cm_ext, fused ? 0 : B * std::max(1L, J / 2) * 2 * n1);
@@ -517,10 +517,10 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   A(w->a_mask, B * n2);
   A(w->a_body, B * n2);
   if (count_only) return bytes;
-  w->g_ck = make_gadget(p.ck_base, (int)p.l_ck, s.r1.Q());
-  w->g_dmux = make_gadget(p.b_dmux, (int)p.l_query, s.r1.Q());
-  w->g_cmux = make_gadget(p.b_cmux, (int)p.l_query, s.r2.Q());
-  w->g_rsk = make_gadget(p.b_rsk, (int)p.l_rsk, s.r3.Q());
+  w->g_ck = make_gadget(p.ck_base, (int)p.l_ck, s.r1);
+  w->g_dmux = make_gadget(p.b_dmux, (int)p.l_query, s.r1);
+  w->g_cmux = make_gadget(p.b_cmux, (int)p.l_query, s.r2);
+  w->g_rsk = make_gadget(p.b_rsk, (int)p.l_rsk, s.r3);
   return bytes;
 }
 
@@ -1131,7 +1131,7 @@ static RepackWs& repack_ws(Server& s, Workspace& w) {
     r->digits.alloc(pairs * 2 * n1 * L);
     r->P.alloc(pairs * 4 * n1);
     r->bsum.alloc(pairs * n1);
-    r->g = make_gadget(p.ck_base, (int)p.l_ck, s.r2.Q());
+    r->g = make_gadget(p.ck_base, (int)p.l_ck, s.r2);
     if (T > w.bmax) r->crot_all.alloc(T * 2 * n1);  // one batch runs in chunks of bmax queries
     w.repack = std::move(r);
   }

@@ -95,7 +95,7 @@ u64* prim_scratch(size_t count) {
 
 Gadget prim_gadget(const DevRing& R, u64 base, uint32_t L) {
   if (base < 2 || L < 1 || L > 64) throw ApiErr(VIA_ERR_INVALID_ARGUMENT, "gadget base must be >= 2 and 1 <= L <= 64");
-  return make_gadget(base, (int)L, R.Q());
+  return make_gadget(base, (int)L, R);
 }
 
 template <class F>
@@ -174,6 +174,32 @@ via_status via_key_switch_dev(const via_ring_desc* ring, uint64_t base, uint32_t
     prim_key_switches(R, gd, key, rlwe, shifts, (long)count, out, s, s + ke, s + ke + mk, s + ke + 2 * mk,
                       s + ke + 2 * mk + dg, st);
     VIA_CUDA(cudaStreamSynchronize(st));
+  });
+}
+
+via_status via_gadget_digits_host(uint64_t q0, uint64_t q1, uint64_t base, uint32_t levels, const uint64_t* coeffs,
+                                  uint64_t count, int64_t* out) {
+  return guarded_prim([&] {
+    if (!coeffs || !out || q0 < 2 || levels < 1 || levels > 64 || base < 2)
+      throw ApiErr(VIA_ERR_INVALID_ARGUMENT, "bad arguments");
+    DevRing R;
+    R.n = 1;
+    R.nl = q1 ? 2 : 1;
+    R.m[0] = make_devmod(q0);
+    R.m[1] = q1 ? make_devmod(q1) : R.m[0];
+    if (q1) {
+      R.q0inv_mod_q1 = h_inv(q0 % q1, q1);
+      if (!R.q0inv_mod_q1) throw ApiErr(VIA_ERR_INVALID_ARGUMENT, "RNS primes are not coprime");
+      R.q0inv_shoup = (u64)(((u128)R.q0inv_mod_q1 << 64) / q1);
+    }
+    const Gadget g = make_gadget(base, (int)levels, R);
+    i64 d[64];
+    for (uint64_t i = 0; i < count; ++i) {
+      const u64 a0 = coeffs[i * R.nl], a1 = R.nl == 2 ? coeffs[i * R.nl + 1] : 0;
+      if (a0 >= q0 || (q1 && a1 >= q1)) throw ApiErr(VIA_ERR_INVALID_ARGUMENT, "residue out of range");
+      decompose_coeff(a0, a1, R, g, d);
+      for (uint32_t k = 0; k < levels; ++k) out[i * levels + k] = d[k];
+    }
   });
 }
 
