@@ -13,6 +13,8 @@
 // multiply-accumulate against the eval-form key (k_mac) -> inverse NTT. Linear
 // steps between products are done in whichever domain saves transforms; since
 // the NTT is exact, the coefficient-form results equal the reference's.
+#include <cooperative_groups.h>
+
 #include <algorithm>
 #include <cmath>
 #include <cstring>
@@ -747,6 +749,89 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fu
   }
 }
 
+// The CMux of k_cmux_fused split over a cluster of four CTAs, for tree levels
+// with too few CMuxes to fill the GPU, where one CMux's latency sets the level's
+// time. CTA r of the cluster takes input half p = r & 1 (mask or body),
+// inverse-transforms its difference, and forward-transforms its digit k = r >> 1;
+// its products with the sample's mask and body (sample p L + L - 1 - k) are
+// reduced mod q into its shared memory. After a cluster barrier, ranks 0 and 1
+// add in[2o] and the four partial masks / bodies, read over distributed shared
+// memory; a second barrier keeps every CTA's shared memory alive until those
+// reads are done. Two transforms per CTA instead of six for one CTA. L = 2 and
+// n <= 2048 (48 KB of static shared memory).
+template <int LOGN>
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
+    k_cmux_cluster(const u64* __restrict__ cur, u64* __restrict__ nxt, KeySel ks, DevRing R, Gadget g) {
+  namespace cg = cooperative_groups;
+  constexpr int n = 1 << LOGN;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  using Fw0 = NttPhase<LOGN, false, 0>;
+  __shared__ u64 ssm[n];    // transform exchanges, then the mask partial
+  __shared__ u64 pbody[n];  // the body partial
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int p = r & 1, k = r >> 1;
+  const int tid = threadIdx.x;
+  const long o = blockIdx.x / 4;
+  const NttTable& T = R.t[0];
+  const DevMod& m = R.m[0];
+  const u64 q = m.q;
+  const u64* a = cur + (2 * o) * 2 * n;
+  const u64* b = a + 2 * n;
+  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
+  u64 e[8];
+  {
+    const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
+    const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const ulonglong2 x = bv[h], y = av[h];
+      e[2 * h] = submod(x.x, y.x, q);
+      e[2 * h + 1] = submod(x.y, y.y, q);
+    }
+  }
+  ntt_inverse_regs<LOGN>(e, tid, T, ssm);
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    u64 c = gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
+    i64 d = gadget_next_digit_small(c, g);
+    if (k) d = gadget_next_digit_small(c, g);
+    e[v] = lift_i64(d, m);
+  }
+  ntt_forward_regs<LOGN>(e, tid, T, ssm);
+  const int smp = p * 2 + 1 - k;  // sample L - 1 - k of half p (L = 2)
+  const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * smp) * n + 8 * tid);
+  const ulonglong2* Kb = Km + n / 2;
+  __syncthreads();  // every thread is done with the transform's exchanges in ssm
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
+    const int s0 = 8 * tid + 2 * h;
+    ssm[s0] = reduce128(mulhi(e[2 * h], km.x), e[2 * h] * km.x, m);
+    ssm[s0 + 1] = reduce128(mulhi(e[2 * h + 1], km.y), e[2 * h + 1] * km.y, m);
+    pbody[s0] = reduce128(mulhi(e[2 * h], kb.x), e[2 * h] * kb.x, m);
+    pbody[s0 + 1] = reduce128(mulhi(e[2 * h + 1], kb.y), e[2 * h + 1] * kb.y, m);
+  }
+  cluster.sync();
+  if (r < 2) {  // rank 0: the output mask, rank 1: the output body
+    u64* parts[4];
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) parts[rr] = cluster.map_shared_rank(r == 0 ? ssm : pbody, rr);
+    u64* out = nxt + o * 2 * n + (long)r * n;
+    for (int x = tid; x < n; x += blockDim.x) {
+      u64 acc = a[(long)r * n + x];
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr) acc = addmod(acc, parts[rr][x], q);
+      out[x] = acc;
+    }
+  }
+  cluster.sync();
+}
+
 // CMux level o < count: fused kernel when the ring has one NTT limb of a
 // supported degree and a small gadget, else diff -> external product -> add.
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
@@ -756,6 +841,17 @@ static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
 
 static void cmux_fused(const DevRing& R, const Gadget& g, const u64* cur, u64* nxt, KeySel ks, long count,
                        cudaStream_t st) {
+  // Levels of at most 64 CMuxes leave most SMs idle: split each CMux over a
+  // four-CTA cluster to cut its latency.
+  if (count <= 64 && g.L == 2 && R.n <= 2048) {
+    switch (R.n) {
+      case 2048: k_cmux_cluster<11><<<(unsigned)(4 * count), 256, 0, st>>>(cur, nxt, ks, R, g); break;
+      case 1024: k_cmux_cluster<10><<<(unsigned)(4 * count), 128, 0, st>>>(cur, nxt, ks, R, g); break;
+      default: k_cmux_cluster<9><<<(unsigned)(4 * count), 64, 0, st>>>(cur, nxt, ks, R, g); break;
+    }
+    VIA_LAUNCHED();
+    return;
+  }
   switch (R.n) {
     case 4096: k_cmux_fused<12><<<(unsigned)count, 512, 0, st>>>(cur, nxt, ks, R, g); break;
     case 2048: k_cmux_fused<11><<<(unsigned)count, 256, 0, st>>>(cur, nxt, ks, R, g); break;
