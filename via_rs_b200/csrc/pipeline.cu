@@ -25,6 +25,9 @@
 
 namespace via {
 
+// Grid size below which k_cascade_mac splits its output masks over more blocks.
+constexpr long CASCADE_SPLIT_BLOCKS = 4 * 148;
+
 // in: npolys polys [p][nl][n_in]; out: digit polys [p][L][nl][n_out] in sample
 // order (slot s = L-1-k holds digit k). n_out = n_in * stride: the input is
 // first embedded at slot 0 (reshape.rs:58), so other positions get digit 0.
@@ -254,14 +257,19 @@ __global__ void k_cascade_reduce(const u64* __restrict__ P, int rank_in, int N, 
 // D: [lwe][idx][L][nl][n_in]; keys: [idx][L][2][nl][n_out]; mask_out:
 // [lwe][R/2][nl][n_out]; bsum: [lwe][nl][n_out]. Block = TT slots x JJ output
 // masks (TT * JJ = 256); the JJ lanes' body partials are summed in shared memory.
+// Small batches give few blocks: the output masks j are then also split over
+// JB blocks (blockIdx.x = slot block * JB + jb), and each block writes its body
+// partial to bpart[lwe][jb][nl][n_out] for k_cascade_bsum to add up.
 __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, const u64* __restrict__ keys, int R,
-                                                     int n_in, int L, int TT, DevRing Rg, u64* __restrict__ mask_out,
-                                                     u64* __restrict__ bsum) {
+                                                     int n_in, int L, int TT, int JB, DevRing Rg,
+                                                     u64* __restrict__ mask_out, u64* __restrict__ bsum,
+                                                     u64* __restrict__ bpart) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
+  const int jb = blockIdx.x % JB;
   const int tl = threadIdx.x % TT, jl = threadIdx.x / TT;
-  const int t = blockIdx.x * TT + tl;
+  const int t = (blockIdx.x / JB) * TT + tl;
   const int l = blockIdx.y;
   const long lwe = blockIdx.z;
   const DevMod& m = Rg.m[l];
@@ -269,7 +277,7 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
   const u64* Dw = D + lwe * R * L * dper + (long)l * n_in + (t >> 1);
   const u64* Kl = keys + (long)l * n_out + t;
   Acc128 ab{0, 0};
-  for (int j = jl; j < half; j += JJ) {
+  for (int j = jl + jb * JJ; j < half; j += JJ * JB) {
     Acc128 am{0, 0};
     const u64* d0 = Dw + (long)j * L * dper;
     const u64* d1 = Dw + (long)(j + half) * L * dper;
@@ -290,8 +298,24 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
   if (jl == 0) {
     u64 acc = part[tl];
     for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
-    bsum[(lwe * nl + l) * n_out + t] = acc;
+    if (JB == 1)
+      bsum[(lwe * nl + l) * n_out + t] = acc;
+    else
+      bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
   }
+}
+
+// bsum[lwe][l][t] = sum over jb of bpart[lwe][jb][l][t] (mod q_l).
+__global__ void k_cascade_bsum(const u64* __restrict__ bpart, int JB, int nl, int n_out, long nlwe, DevRing Rg,
+                               u64* __restrict__ bsum) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  const long per = (long)nl * n_out;
+  if (gid >= nlwe * per) return;
+  const long lwe = gid / per, rem = gid % per;
+  const u64 q = Rg.m[rem / n_out].q;
+  u64 acc = 0;
+  for (int jb = 0; jb < JB; ++jb) acc = addmod(acc, bpart[(lwe * JB + jb) * per + rem], q);
+  bsum[gid] = acc;
 }
 
 // body_out[lwe] = embed_at(body_in[lwe], N_out, 0) - bsum[lwe] (coefficient form).
@@ -412,6 +436,7 @@ struct Workspace {
   int bmax = 1;              // queries the buffers are sized for
   // Cascade.
   DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
+  DevBuf c_bpart;  // k_cascade_mac body partials when the masks are split over blocks
   // RLWE -> RGSW.
   DevBuf g_digits, g_gp, rgsw_q1;  // rgsw_q1: [q][nbits][2L][2][nl][n1]
   DevBuf rgsw_q2;                  // all bits mod-switched to q2: [q][nbits][2L][2][n1]
@@ -483,6 +508,8 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   A(w->c_digits, nlwe * (s.r1.ntt ? 1 : 2) * n1 * Lck * nl);
   A(w->c_P, s.r1.ntt ? 0 : nlwe * 2 * n1 * 2 * nl);
   A(w->c_bsum, nlwe * n1 * nl);
+  // A split grid has at most CASCADE_SPLIT_BLOCKS blocks of at most 256 slots.
+  A(w->c_bpart, s.r1.ntt ? (long)CASCADE_SPLIT_BLOCKS * 256 : 0);
   A(w->c_rlwe, nlwe * 2 * n1 * nl);
   A(w->g_digits, nlwe * Lck * nl * n1);
   A(w->g_gp, nlwe * 2 * nl * n1);
@@ -604,10 +631,20 @@ static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cu
       decompose(R, w.g_ck, mi, n_in, 1, polys, w.c_digits.p, st);
       if (n_in > 1) to_eval(R, w.c_digits.p, n_in, polys * L * nl, st);
       int jj = std::min(rank_in / 2, 8), tt = std::min(n_out, 256 / jj);
-      dim3 grid((unsigned)(n_out / tt), (unsigned)nl, (unsigned)nlwe);
-      k_cascade_mac<<<grid, 256, 0, st>>>(w.c_digits.p, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, R, mo,
-                                          w.c_bsum.p);
+      // Split the output masks over JB blocks while the grid is below ~4 blocks
+      // per SM and every block keeps at least one mask per thread row.
+      const long base = (long)(n_out / tt) * nl * nlwe;
+      const int iters = (rank_in / 2 + 256 / tt - 1) / (256 / tt);
+      int JB = 1;
+      while (JB * 2 <= iters && base * JB * 2 <= CASCADE_SPLIT_BLOCKS) JB *= 2;
+      dim3 grid((unsigned)(n_out / tt * JB), (unsigned)nl, (unsigned)nlwe);
+      k_cascade_mac<<<grid, 256, 0, st>>>(w.c_digits.p, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R,
+                                          mo, w.c_bsum.p, w.c_bpart.p);
       VIA_LAUNCHED();
+      if (JB > 1) {
+        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(w.c_bpart.p, JB, nl, n_out, nlwe, R, w.c_bsum.p);
+        VIA_LAUNCHED();
+      }
     } else {
       gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), w.c_P.p,
                      w.c_digits.p, st);
