@@ -149,6 +149,10 @@ struct Gadget {
   Div64 dq, dq1;  // mode 0: Q; mode 1: q0 and q1
   u64 q0, q1;     // mode 1 limbs
   Div64 dbc;      // B^c, for the two-chunk split when S >= 2^64
+  // Digit extraction in 32-bit pieces of c32 digits (B^c32 < 2^32).
+  int c32;
+  Div64 dc32;     // B^c32
+  u32 bmagic;     // floor((2^32 - 1) / B)
 };
 
 inline Gadget make_gadget(u64 base, int L, u128 Q, u64 q0 = 0, u64 q1 = 0) {
@@ -200,6 +204,15 @@ inline Gadget make_gadget(u64 base, int L, u128 Q, u64 q0 = 0, u64 q1 = 0) {
     g.mode = 2;
   }
   if (c < L) g.dbc = make_div64((u64)Bc);
+  int c32 = 0;
+  u64 b32 = 1;
+  while (c32 < L && (u128)b32 * base < ((u128)1 << 32)) {
+    b32 *= base;
+    ++c32;
+  }
+  g.c32 = c32;
+  g.dc32 = make_div64(b32);
+  g.bmagic = (u32)(0xFFFFFFFFull / base);
   return g;
 }
 
@@ -352,12 +365,81 @@ __host__ __device__ __forceinline__ i64 gadget_next_digit_small(u64& cur, const 
   return (i64)r;
 }
 
+__host__ __device__ __forceinline__ u32 mulhi32(u32 a, u32 b) {
+#ifdef __CUDA_ARCH__
+  return __umulhi(a, b);
+#else
+  return (u32)(((u64)a * b) >> 32);
+#endif
+}
+
+// The balanced base-B digits of a scaled value v < B^L, LSB first, passed to
+// f(k, d). v is cut into 32-bit pieces of c32 digits (one 128-by-64 division
+// per piece but the last); each piece plus the carry of the previous one
+// (at most B^c32 < 2^32) yields its digits with 32-bit divisions by B. The
+// carry out of the top digit is dropped (the digits depend on v mod B^L).
+template <class F>
+__host__ __device__ __forceinline__ void for_each_digit(u128 v, const Gadget& g, F&& f) {
+  const u32 B = (u32)g.base, half = (u32)g.half_base;
+  u32 carry = 0;
+  for (int k = 0; k < g.L;) {
+    u32 x;
+    if (k + g.c32 < g.L) {
+      u64 rem;
+      v = div128by64(v, g.dc32, rem);
+      x = (u32)rem + carry;
+    } else {
+      x = (u32)v + carry;
+    }
+    const int cnt = g.L - k < g.c32 ? g.L - k : g.c32;
+    for (int i = 0; i < cnt; ++i, ++k) {
+      u32 q = mulhi32(x, g.bmagic);  // floor(x / B) - {0, 1, 2}
+      u64 r = (u64)x - (u64)q * B;
+      if (r >= B) {
+        r -= B;
+        ++q;
+      }
+      if (r >= B) {
+        r -= B;
+        ++q;
+      }
+      if (r > half) {
+        f(k, (i64)r - (i64)B);
+        x = q + 1;
+      } else {
+        f(k, (i64)r);
+        x = q;
+      }
+    }
+    carry = x;
+  }
+}
+
+// The next balanced digit of a running 32-bit value x < 2^32 (LSB first).
+__host__ __device__ __forceinline__ i64 gadget_next_digit32(u32& x, const Gadget& g) {
+  const u32 B = (u32)g.base;
+  u32 q = mulhi32(x, g.bmagic);
+  u64 r = (u64)x - (u64)q * B;
+  if (r >= B) {
+    r -= B;
+    ++q;
+  }
+  if (r >= B) {
+    r -= B;
+    ++q;
+  }
+  if (r > g.half_base) {
+    x = q + 1;
+    return (i64)r - (i64)B;
+  }
+  x = q;
+  return (i64)r;
+}
+
 // Digits of one coefficient given its residues (nl limbs). Writes L signed
 // digits, d[k] = k-th least significant (pairs with sample L-1-k).
 __host__ __device__ inline void decompose_coeff(u64 a0, u64 a1, const DevRing& R, const Gadget& g, i64* d) {
-  u64 cur, hi;
-  gadget_chunks(gadget_scaled(a0, a1, R, g), g, cur, hi);
-  for (int k = 0; k < g.L; ++k) d[k] = gadget_next_digit(cur, hi, k, g);
+  for_each_digit(gadget_scaled(a0, a1, R, g), g, [&](int k, i64 v) { d[k] = v; });
 }
 
 }  // namespace via

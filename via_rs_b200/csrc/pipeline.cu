@@ -40,19 +40,18 @@ __global__ void k_decompose(const u64* __restrict__ in, int n_in, int stride, lo
   const int nl = R.nl;
   const u64* src = in + p * nl * n_in;
   u64 a0 = src[i], a1 = nl == 2 ? src[n_in + i] : 0;
-  u64 cur, hi;
-  gadget_chunks(gadget_scaled(a0, a1, R, g), g, cur, hi);
   const int n_out = n_in * stride;
-  u64* dst = out + p * (long)g.L * nl * n_out + (long)i * stride;
-  for (int k = 0; k < g.L; ++k) {
-    const i64 d = gadget_next_digit(cur, hi, k, g);
-    const int s = g.L - 1 - k;
+  const long step = (long)nl * n_out;
+  // Digit k goes to sample slot L - 1 - k.
+  u64* o = out + p * (long)g.L * step + (long)(g.L - 1) * step + (long)i * stride;
+  for_each_digit(gadget_scaled(a0, a1, R, g), g, [&](int, i64 d) {
     for (int l = 0; l < nl; ++l) {
-      u64* o = dst + ((long)s * nl + l) * n_out;
-      o[0] = lift_i64(d, R.m[l]);
-      for (int z = 1; z < stride; ++z) o[z] = 0;
+      u64* ol = o + (long)l * n_out;
+      ol[0] = lift_i64(d, R.m[l]);
+      for (int z = 1; z < stride; ++z) ol[z] = 0;
     }
-  }
+    o -= step;
+  });
 }
 
 // Which eval-form key samples output o multiplies: K_o = base + ((o / div) % mod) * stride.
@@ -751,11 +750,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fu
     for (int v = 0; v < 8; ++v) dcur[v] = (u32)gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
     for (int k = 0; k < L; ++k) {
 #pragma unroll
-      for (int v = 0; v < 8; ++v) {
-        u64 c = dcur[v];
-        e[v] = lift_i64(gadget_next_digit_small(c, g), m);
-        dcur[v] = (u32)c;
-      }
+      for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit32(dcur[v], g), m);
       ntt_forward_regs<LOGN>(e, tid, T, ssm);
       const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * (p * L + L - 1 - k)) * n + 8 * tid);
       const ulonglong2* Kb = Km + n / 2;
@@ -834,9 +829,9 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
   __syncthreads();
 #pragma unroll
   for (int v = 0; v < 8; ++v) {
-    u64 c = gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
-    i64 d = gadget_next_digit_small(c, g);
-    if (k) d = gadget_next_digit_small(c, g);
+    u32 c = (u32)gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
+    i64 d = gadget_next_digit32(c, g);
+    if (k) d = gadget_next_digit32(c, g);
     e[v] = lift_i64(d, m);
   }
   ntt_forward_regs<LOGN>(e, tid, T, ssm);
