@@ -558,6 +558,7 @@ FdTile from_abi(const via_scan_tile& t) { return FdTile{(int)t.n_max, (int)t.sta
 
 void autotune_scan(Server& s, Workspace& w, const std::vector<int>& sizes, const char* cache_path,
                    std::vector<via_scan_tuning>* out) {
+  std::unique_lock<std::shared_mutex> plan(s.plan_mu);
   if (!s.tensor_fd()) {  // schoolbook rings have no tiles
     if (out)
       for (int nq : sizes) out->push_back(via_scan_tuning{(uint32_t)nq, {0, 0, 0, 0}, 0.f, 0.f, 0, 0});

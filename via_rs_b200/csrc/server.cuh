@@ -3,6 +3,7 @@
 #pragma once
 #include <memory>
 #include <mutex>
+#include <shared_mutex>
 #include <string>
 #include <vector>
 
@@ -69,6 +70,9 @@ struct Server {
   std::unique_ptr<Workspace, WorkspaceDeleter> ws;
   std::mutex mu;  // one in-flight answer per handle (the workspace is shared)
   int plan_gen = 0;  // bumped when the scan tiles change; captured graphs of older plans are dropped
+  // Guards fd.tuned and plan_gen: the autotuner holds it exclusively, service
+  // workers (which do not take `mu`) hold it shared while they enqueue a batch.
+  std::shared_mutex plan_mu;
   bool tensor_fd() const { return fd.planes != nullptr; }
   ~Server();
 };

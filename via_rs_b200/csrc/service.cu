@@ -118,6 +118,7 @@ void Service::launch(Lane& L) {
     L.batch.push_back(r);
   }
   try {
+    std::shared_lock<std::shared_mutex> plan(s->plan_mu);  // the scan tiles stay fixed while this batch is enqueued
     u64* d_in = L.d_in ? L.d_in->p : ws_query(*L.ws);
     VIA_CUDA(cudaMemcpyAsync(d_in, L.h_in, (size_t)n * unit_len * 8, cudaMemcpyHostToDevice, L.stream));
     if (via_b)
