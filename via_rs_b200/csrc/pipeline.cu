@@ -453,9 +453,16 @@ struct Workspace {
   std::unique_ptr<struct RepackWs> repack;  // VIA-B buffers, made on the first batch answer
   cudaStream_t capture = nullptr;           // stream the answer graphs are captured on
   int graphs_gen = 0;                       // Server::plan_gen the graphs were captured under
+  // A one-query answer expands its CMux / CRot bits on `side`, concurrently with
+  // the DMux tree and the database scan on the answer's stream (fork / join).
+  cudaStream_t side = nullptr;
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   ~Workspace() {
     for (auto& g : graphs) cudaGraphExecDestroy(g.second);
     if (capture) cudaStreamDestroy(capture);
+    if (side) cudaStreamDestroy(side);
+    if (ev_fork) cudaEventDestroy(ev_fork);
+    if (ev_join) cudaEventDestroy(ev_join);
   }
 };
 
@@ -508,7 +515,8 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   A(w->c_P, s.r1.ntt ? 0 : nlwe * 2 * n1 * 2 * nl);
   A(w->c_bsum, nlwe * n1 * nl);
   // A split grid has at most CASCADE_SPLIT_BLOCKS blocks of at most 256 slots.
-  A(w->c_bpart, s.r1.ntt ? (long)CASCADE_SPLIT_BLOCKS * 256 : 0);
+  // Two halves: the answer's stream and the side stream expand concurrently.
+  A(w->c_bpart, s.r1.ntt ? 2L * CASCADE_SPLIT_BLOCKS * 256 : 0);
   A(w->c_rlwe, nlwe * 2 * n1 * nl);
   A(w->g_digits, nlwe * Lck * nl * n1);
   A(w->g_gp, nlwe * 2 * nl * n1);
@@ -556,6 +564,9 @@ std::unique_ptr<Workspace, WorkspaceDeleter> workspace_make(Server& s, int bmax)
   std::unique_ptr<Workspace, WorkspaceDeleter> w(new Workspace());
   workspace_build(s, bmax, w.get(), false);
   VIA_CUDA(cudaStreamCreateWithFlags(&w->capture, cudaStreamNonBlocking));
+  VIA_CUDA(cudaStreamCreateWithFlags(&w->side, cudaStreamNonBlocking));
+  VIA_CUDA(cudaEventCreateWithFlags(&w->ev_fork, cudaEventDisableTiming));
+  VIA_CUDA(cudaEventCreateWithFlags(&w->ev_join, cudaEventDisableTiming));
   return w;
 }
 
@@ -611,15 +622,27 @@ static void mod_switch(const DevRing& S, const u64* in, const DevRing& D, u64* o
   VIA_LAUNCHED();
 }
 
-// Step 1: QueryDecomp for nq queries -> rgsw_q1 [q][nbits][2L][2][nl][n1] (coefficient form).
-static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cudaStream_t st) {
+// Step 1: QueryDecomp (query_decomp.rs:39-95) of `nlwe` consecutive LWEs, the
+// first being LWE lwe0 of the workspace (LWE-indexed buffers are used from that
+// LWE's region on), forming the RGSWs of `nbits` query bits starting at bit
+// bit0 -> rgsw_q1 [bit][2L][2][nl][n1] (coefficient form). `bpart` is this
+// call's k_cascade_mac scratch. Disjoint (lwe0, nlwe) ranges may run
+// concurrently on different streams.
+static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long lwe0, long nlwe, long bit0,
+                               long nbits, u64* bpart, cudaStream_t st) {
   const via_params& p = s.prm;
   const DevRing& R = s.r1;
   const int n1 = p.n1, nl = R.nl, L = p.l_ck;
-  const long nlwe = w.nlwe * nq;
-  k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query, n1, nl, nlwe, w.c_masks_a.p, w.c_body_a.p);
+  const long lwe_n = (long)n1 * nl;  // per-LWE region of the mask / body / bsum buffers
+  const long rgsw1 = 2L * p.l_query * 2 * nl * n1;
+  u64 *mi = w.c_masks_a.p + lwe0 * lwe_n, *mo = w.c_masks_b.p + lwe0 * lwe_n;
+  u64 *bi = w.c_body_a.p + lwe0 * lwe_n, *bo = w.c_body_b.p + lwe0 * lwe_n;
+  u64* digits = w.c_digits.p + lwe0 * (R.ntt ? 1 : 2) * n1 * L * nl;
+  u64* cP = R.ntt ? nullptr : w.c_P.p + lwe0 * 2 * n1 * 2 * nl;
+  u64* bsum = w.c_bsum.p + lwe0 * lwe_n;
+  u64* rlwe = w.c_rlwe.p + lwe0 * 2 * lwe_n;
+  k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query + lwe0 * (long)lwe_len(p), n1, nl, nlwe, mi, bi);
   VIA_LAUNCHED();
-  u64 *mi = w.c_masks_a.p, *mo = w.c_masks_b.p, *bi = w.c_body_a.p, *bo = w.c_body_b.p;
   const u64 step_len = (u64)2 * n1 * L * 2 * nl;
   int k = 0;
   for (int n_in = 1; n_in < n1; n_in <<= 1, ++k) {
@@ -627,8 +650,8 @@ static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cu
     const long polys = nlwe * rank_in;
     if (R.ntt) {
       // Digits at the input degree; see k_cascade_mac for the repeated slots.
-      decompose(R, w.g_ck, mi, n_in, 1, polys, w.c_digits.p, st);
-      if (n_in > 1) to_eval(R, w.c_digits.p, n_in, polys * L * nl, st);
+      decompose(R, w.g_ck, mi, n_in, 1, polys, digits, st);
+      if (n_in > 1) to_eval(R, digits, n_in, polys * L * nl, st);
       int jj = std::min(rank_in / 2, 8), tt = std::min(n_out, 256 / jj);
       // Split the output masks over JB blocks while the grid is below ~4 blocks
       // per SM and every block keeps at least one mask per thread row.
@@ -637,36 +660,42 @@ static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cu
       int JB = 1;
       while (JB * 2 <= iters && base * JB * 2 <= CASCADE_SPLIT_BLOCKS) JB *= 2;
       dim3 grid((unsigned)(n_out / tt * JB), (unsigned)nl, (unsigned)nlwe);
-      k_cascade_mac<<<grid, 256, 0, st>>>(w.c_digits.p, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R,
-                                          mo, w.c_bsum.p, w.c_bpart.p);
+      k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
+                                          bsum, bpart);
       VIA_LAUNCHED();
       if (JB > 1) {
-        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(w.c_bpart.p, JB, nl, n_out, nlwe, R, w.c_bsum.p);
+        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bpart, JB, nl, n_out, nlwe, R, bsum);
         VIA_LAUNCHED();
       }
     } else {
-      gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), w.c_P.p,
-                     w.c_digits.p, st);
+      gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), cP,
+                     digits, st);
       const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
-      k_cascade_reduce<<<blocks(items), 256, 0, st>>>(w.c_P.p, rank_in, n_out, nl, nlwe, R, mo, w.c_bsum.p);
+      k_cascade_reduce<<<blocks(items), 256, 0, st>>>(cP, rank_in, n_out, nl, nlwe, R, mo, bsum);
       VIA_LAUNCHED();
     }
     from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
-    from_eval(R, w.c_bsum.p, n_out, nlwe * nl, st);
-    k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, w.c_bsum.p, n_in, nl, nlwe, R, bo);
+    from_eval(R, bsum, n_out, nlwe * nl, st);
+    k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, bsum, n_in, nl, nlwe, R, bo);
     VIA_LAUNCHED();
     std::swap(mi, mo);
     std::swap(bi, bo);
   }
-  k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, w.c_rlwe.p);
+  k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, rlwe);
   VIA_LAUNCHED();
   // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178); the
   // final rank-1 masks are already contiguous [lwe][nl][n1] in `mi`.
-  gadget_product(R, w.g_ck, mi, n1, 1, 1, nlwe, keys_shared(s.conv_eval.p), w.g_gp.p, w.g_digits.p, st);
-  from_eval(R, w.g_gp.p, n1, nlwe * 2 * nl, st);
-  k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(w.c_rlwe.p, w.g_gp.p, (int)p.l_query, w.nbits * nq, n1,
-                                                               nl, R, w.rgsw_q1.p);
+  u64* gp = w.g_gp.p + lwe0 * 2 * lwe_n;
+  gadget_product(R, w.g_ck, mi, n1, 1, 1, nlwe, keys_shared(s.conv_eval.p), gp, w.g_digits.p + lwe0 * L * lwe_n, st);
+  from_eval(R, gp, n1, nlwe * 2 * nl, st);
+  k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(rlwe, gp, (int)p.l_query, nbits, n1, nl, R,
+                                                               w.rgsw_q1.p + bit0 * rgsw1);
   VIA_LAUNCHED();
+}
+
+// Step 1 for the whole batch: nq queries -> rgsw_q1 [q][nbits][2L][2][nl][n1].
+static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cudaStream_t st) {
+  query_decomp_range(s, w, d_query, 0, w.nlwe * nq, 0, (long)w.nbits * nq, w.c_bpart.p, st);
 }
 
 // ext[o] = bit_o (x) cts[o] for `count` RLWEs (coefficient form); result in the
@@ -992,16 +1021,36 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   auto copy_out = [&](const u64* src, size_t count) {
     VIA_CUDA(cudaMemcpyAsync(dump, src, count * 8, cudaMemcpyDeviceToDevice, st));
   };
-  // ---- Step 1: QueryDecomp.
-  query_decomp(s, w, d_query, nq, st);
-  if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
-  if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
+  // One query answered to the end: the CMux / CRot bits' expansion (their
+  // cascades, RGSWs and q1 -> q2 switch) runs on the side stream while the DMux
+  // tree and the database scan run on `st`; `st` waits for it before the CMux
+  // tree. Their LWEs and buffer regions are disjoint from the DMux bits'.
+  const bool split = nq == 1 && (stop_stage == 0 || stop_stage == STOP_AFTER_CROT) && nd > 0 && w.nbits > nd &&
+                     s.r1.ntt;
+  if (split) {
+    const long lwe_d = (long)nd * L;  // the DMux bits' LWEs come first (query.rs order)
+    VIA_CUDA(cudaEventRecord(w.ev_fork, st));
+    VIA_CUDA(cudaStreamWaitEvent(w.side, w.ev_fork, 0));
+    query_decomp_range(s, w, d_query, lwe_d, w.nlwe - lwe_d, nd, w.nbits - nd,
+                       w.c_bpart.p + CASCADE_SPLIT_BLOCKS * 256, w.side);
+    mod_switch(s.r1, w.rgsw_q1.p + nd * rgsw1, s.r2, w.rgsw_q2.p + nd * rgsw2, (w.nbits - nd) * 2 * L * 2, n1,
+               w.side);
+    to_eval(s.r2, w.rgsw_q2.p + nd * rgsw2, n1, (w.nbits - nd) * 2 * L * 2, w.side);
+    VIA_CUDA(cudaEventRecord(w.ev_join, w.side));
+    query_decomp_range(s, w, d_query, 0, lwe_d, 0, nd, w.c_bpart.p, st);
+    to_eval(s.r1, w.rgsw_q1.p, n1, (long)nd * 2 * L * 2 * nl, st);
+  } else {
+    // ---- Step 1: QueryDecomp.
+    query_decomp(s, w, d_query, nq, st);
+    if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
+    if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
 
-  // ---- mod_switch_rgsw q1 -> q2 of every bit (convert.rs:223-240; only the
-  // CMux / CRot bits are used at q2), then eval form for both moduli.
-  mod_switch(s.r1, w.rgsw_q1.p, s.r2, w.rgsw_q2.p, B * w.nbits * 2 * L * 2, n1, st);
-  to_eval(s.r2, w.rgsw_q2.p, n1, B * w.nbits * 2 * L * 2, st);
-  to_eval(s.r1, w.rgsw_q1.p, n1, B * w.nbits * 2 * L * 2 * nl, st);
+    // ---- mod_switch_rgsw q1 -> q2 of every bit (convert.rs:223-240; only the
+    // CMux / CRot bits are used at q2), then eval form for both moduli.
+    mod_switch(s.r1, w.rgsw_q1.p, s.r2, w.rgsw_q2.p, B * w.nbits * 2 * L * 2, n1, st);
+    to_eval(s.r2, w.rgsw_q2.p, n1, B * w.nbits * 2 * L * 2, st);
+    to_eval(s.r1, w.rgsw_q1.p, n1, B * w.nbits * 2 * L * 2 * nl, st);
+  }
 
   // ---- Step 2: DMux tree at q1 from the trivial RLWE(0, delta) (answer.rs:181-191).
   {
@@ -1036,6 +1085,8 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
     from_eval(s.r2, dump, n1, 2 * J, st);
     return;
   }
+
+  if (split) VIA_CUDA(cudaStreamWaitEvent(st, w.ev_join, 0));  // the CMux / CRot RGSWs are ready
 
   // ---- Step 5: CMux tree (mux.rs:167-198), level by level in the eval domain:
   // diff = in[2j+1] - in[2j] (eval) -> coeff -> gadget product -> out[j] = in[2j] + ext.
