@@ -219,6 +219,18 @@ __global__ void k_lwe_to_mlwe(const u64* __restrict__ q, int n1, int nl, long nl
   }
 }
 
+// Regroups a batch's query LWEs: every query's first lwe_a LWEs (its DMux
+// bits), query by query, then the rest of every query. Element-wise copy.
+__global__ void k_permute_lwes(const u64* __restrict__ q, long nq, long n_lwe, long lwe_a, long lwe_len,
+                               u64* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= nq * n_lwe * lwe_len) return;
+  const long e = gid % lwe_len, lw = gid / lwe_len;
+  const long qi = lw / n_lwe, j = lw % n_lwe;
+  const long dst = j < lwe_a ? qi * lwe_a + j : nq * lwe_a + qi * (n_lwe - lwe_a) + (j - lwe_a);
+  out[dst * lwe_len + e] = q[gid];
+}
+
 // After the step MAC: P [lwe][RANK_IN][2][nl][N] (eval). Produces
 // masks_out[lwe][j] = -(P[j].mask + P[j+R].mask) for j < R and
 // bsum[lwe] = sum_idx P[idx].body.
@@ -437,8 +449,11 @@ struct Workspace {
   DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
   DevBuf c_bpart;  // k_cascade_mac body partials when the masks are split over blocks
   // RLWE -> RGSW.
-  DevBuf g_digits, g_gp, rgsw_q1;  // rgsw_q1: [q][nbits][2L][2][nl][n1]
-  DevBuf rgsw_q2;                  // all bits mod-switched to q2: [q][nbits][2L][2][n1]
+  // RGSWs grouped by use: the DMux bits of every query ([q][nd]), then the
+  // CMux and CRot bits ([q][nbits - nd]), each [2L][2][nl][n1] at q1.
+  DevBuf g_digits, g_gp, rgsw_q1;
+  DevBuf rgsw_q2;  // the same layout switched to q2: [2L][2][n1] per bit
+  DevBuf q_perm;   // a batch's query LWEs in that grouped order (batches of two or more)
   // DMux.
   DevBuf dm_a, dm_b, dm_digits, dm_ext;
   // FirstDim / CMux.
@@ -550,6 +565,7 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   A(w->rs_gp, B * d * 2 * n2);
   A(w->rs_acc, B * 2 * n2);
   A(w->q_in, nlwe * lwe_len(p));
+  A(w->q_perm, B > 1 ? nlwe * (long)lwe_len(p) : 0);
   A(w->a_mask, B * n2);
   A(w->a_body, B * n2);
   if (count_only) return bytes;
@@ -693,10 +709,6 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
   VIA_LAUNCHED();
 }
 
-// Step 1 for the whole batch: nq queries -> rgsw_q1 [q][nbits][2L][2][nl][n1].
-static void query_decomp(Server& s, Workspace& w, const u64* d_query, int nq, cudaStream_t st) {
-  query_decomp_range(s, w, d_query, 0, w.nlwe * nq, 0, (long)w.nbits * nq, w.c_bpart.p, st);
-}
 
 // ext[o] = bit_o (x) cts[o] for `count` RLWEs (coefficient form); result in the
 // eval domain unless `to_coeff`. The RGSW of output o is selected by `rgsw`.
@@ -1021,29 +1033,39 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   auto copy_out = [&](const u64* src, size_t count) {
     VIA_CUDA(cudaMemcpyAsync(dump, src, count * 8, cudaMemcpyDeviceToDevice, st));
   };
-  // One query answered to the end: the CMux / CRot bits' expansion (their
-  // cascades, RGSWs and q1 -> q2 switch) runs on the side stream while the DMux
-  // tree and the database scan run on `st`; `st` waits for it before the CMux
-  // tree. Their LWEs and buffer regions are disjoint from the DMux bits'.
-  const bool split = nq == 1 && (stop_stage == 0 || stop_stage == STOP_AFTER_CROT) && nd > 0 && w.nbits > nd &&
-                     s.r1.ntt;
+  // ---- Step 1: QueryDecomp. The LWEs are taken grouped by use (every query's
+  // DMux bits, then every query's CMux and CRot bits), so the RGSWs come out in
+  // the grouped layout of rgsw_q1 and each group is one contiguous range.
+  const long nb = w.nbits - nd;                 // CMux + CRot bits per query
+  const long lwe_a = (long)nd * L, nlwe_all = w.nlwe * B;
+  const u64* qsrc = d_query;
+  if (B > 1) {
+    const long ll = (long)lwe_len(p);
+    k_permute_lwes<<<blocks(nlwe_all * ll), 256, 0, st>>>(d_query, B, w.nlwe, lwe_a, ll, w.q_perm.p);
+    VIA_LAUNCHED();
+    qsrc = w.q_perm.p;
+  }
+  u64* const rgsw_b1 = w.rgsw_q1.p + B * nd * rgsw1;  // the CMux / CRot bits' group
+  u64* const rgsw_b2 = w.rgsw_q2.p + B * nd * rgsw2;
+  // Answers that run to the end expand the CMux / CRot bits (their cascades,
+  // RGSWs and q1 -> q2 switch) on the side stream while the DMux tree and the
+  // database scan run on `st`; `st` waits for them before the CMux tree. The
+  // two groups' LWEs, buffer regions and scratch are disjoint.
+  const bool split = (stop_stage == 0 || stop_stage == STOP_AFTER_CROT) && nd > 0 && nb > 0 && s.r1.ntt;
   if (split) {
-    const long lwe_d = (long)nd * L;  // the DMux bits' LWEs come first (query.rs order)
     VIA_CUDA(cudaEventRecord(w.ev_fork, st));
     VIA_CUDA(cudaStreamWaitEvent(w.side, w.ev_fork, 0));
-    query_decomp_range(s, w, d_query, lwe_d, w.nlwe - lwe_d, nd, w.nbits - nd,
+    query_decomp_range(s, w, qsrc, B * lwe_a, nlwe_all - B * lwe_a, B * nd, B * nb,
                        w.c_bpart.p + CASCADE_SPLIT_BLOCKS * 256, w.side);
-    mod_switch(s.r1, w.rgsw_q1.p + nd * rgsw1, s.r2, w.rgsw_q2.p + nd * rgsw2, (w.nbits - nd) * 2 * L * 2, n1,
-               w.side);
-    to_eval(s.r2, w.rgsw_q2.p + nd * rgsw2, n1, (w.nbits - nd) * 2 * L * 2, w.side);
+    mod_switch(s.r1, rgsw_b1, s.r2, rgsw_b2, B * nb * 2 * L * 2, n1, w.side);
+    to_eval(s.r2, rgsw_b2, n1, B * nb * 2 * L * 2, w.side);
     VIA_CUDA(cudaEventRecord(w.ev_join, w.side));
-    query_decomp_range(s, w, d_query, 0, lwe_d, 0, nd, w.c_bpart.p, st);
-    to_eval(s.r1, w.rgsw_q1.p, n1, (long)nd * 2 * L * 2 * nl, st);
+    query_decomp_range(s, w, qsrc, 0, B * lwe_a, 0, B * nd, w.c_bpart.p, st);
+    to_eval(s.r1, w.rgsw_q1.p, n1, B * nd * 2 * L * 2 * nl, st);
   } else {
-    // ---- Step 1: QueryDecomp.
-    query_decomp(s, w, d_query, nq, st);
+    query_decomp_range(s, w, qsrc, 0, nlwe_all, 0, B * w.nbits, w.c_bpart.p, st);
     if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
-    if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);
+    if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);  // one query: bit order
 
     // ---- mod_switch_rgsw q1 -> q2 of every bit (convert.rs:223-240; only the
     // CMux / CRot bits are used at q2), then eval form for both moduli.
@@ -1064,7 +1086,7 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
     u64 *in = w.dm_a.p, *out = w.dm_b.p;
     for (int i = 0; i < nd; ++i) {
       const long active = 1L << i;  // per query
-      KeySel bit{w.rgsw_q1.p + i * rgsw1, active, B, w.nbits * rgsw1};
+      KeySel bit{w.rgsw_q1.p + i * rgsw1, active, B, nd * rgsw1};
       external_products(s.r1, w.g_dmux, bit, in, B * active, w.dm_digits.p, w.dm_ext.p, true, st);
       k_dmux_combine<<<blocks(B * active * 2 * nl * n1), 256, 0, st>>>(out, in, w.dm_ext.p, B * active, n1, nl, s.r1);
       VIA_LAUNCHED();
@@ -1093,7 +1115,7 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   u64* cur = w.fd_out.p;
   for (int i = 0; i < nc; ++i) {
     const long half = (J >> i) / 2;  // CMuxes per query at this level
-    KeySel bit{w.rgsw_q2.p + (nd + i) * rgsw2, half, B, w.nbits * rgsw2};
+    KeySel bit{rgsw_b2 + i * rgsw2, half, B, nb * rgsw2};
     u64* nxt = cur == w.fd_out.p ? w.cm_b.p : w.fd_out.p;  // ping-pong between fd_out and cm_b
     if (cmux_fused_ok(s.r2, w.g_cmux)) {
       cmux_fused(s.r2, w.g_cmux, cur, nxt, bit, B * half, st);
@@ -1118,7 +1140,7 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   for (int i = 0; i < nr; ++i) {
     k_crot_diff_batch<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, n1, n1 - (1 << i), B, s.r2.m[0], w.cr_diff.p);
     VIA_LAUNCHED();
-    KeySel bit{w.rgsw_q2.p + (nd + nc + i) * rgsw2, 1, B, w.nbits * rgsw2};
+    KeySel bit{rgsw_b2 + (nc + i) * rgsw2, 1, B, nb * rgsw2};
     external_products(s.r2, w.g_cmux, bit, w.cr_diff.p, B, w.cr_digits.p, w.cr_ext.p, true, st);
     k_rlwe_addsub<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, w.cr_ct.p, 1, w.cr_ext.p, 1, +1, B, n1, 1, s.r2);
     VIA_LAUNCHED();
