@@ -130,7 +130,9 @@ __device__ __forceinline__ u64 ntt_canonical(u64 x, const NttTable& T) {
 // phase-0 layout (NttPhase<LOGN,false,0>::index); leaves them (exact) in the
 // layout of the last phase. `ssm` is an n-residue shared-memory exchange area
 // of one segment, addressed through swz().
-template <int LOGN, int P = 0>
+// With LAZY the outputs stay below (1 + 2 LOGN) q instead of being reduced,
+// for callers that reduce a sum of products once at the end.
+template <int LOGN, int P = 0, bool LAZY = false>
 __device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const NttTable& T, u64* ssm) {
   using Ph = NttPhase<LOGN, false, P>;
   constexpr int NPH = (LOGN + 2) / 3;
@@ -143,8 +145,8 @@ __device__ __forceinline__ void ntt_forward_regs(u64 (&e)[8], int tid, const Ntt
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) e[v] = ssm[swz(Nx::index(v, tid))];
-    ntt_forward_regs<LOGN, P + 1>(e, tid, T, ssm);
-  } else {
+    ntt_forward_regs<LOGN, P + 1, LAZY>(e, tid, T, ssm);
+  } else if constexpr (!LAZY) {
 #pragma unroll
     for (int v = 0; v < 8; ++v) e[v] = ntt_canonical(e[v], T);
   }

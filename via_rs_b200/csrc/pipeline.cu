@@ -731,7 +731,8 @@ static void external_products(const DevRing& R, const Gadget& g, KeySel rgsw, co
 // cur: [count*2][2][n]; nxt: [count][2][n]; the RGSW of CMux o ([2L][2][n],
 // eval) is picked by `ks`. The digits never leave registers.
 // Sum of products of residues below 2^40: each product's high word is below
-// 2^16, so up to 2^16 products fit a 32-bit high word (callers check q < 2^40).
+// 2^16, so up to 2^16 products fit a 32-bit high word. The digit transforms'
+// lazy outputs stay below (1 + 2 LOGN) q < 2^40 for q < 2^35 (cmux_fused_ok).
 // Three registers instead of four.
 struct Acc96 {
   u64 lo;
@@ -792,7 +793,8 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fu
     for (int k = 0; k < L; ++k) {
 #pragma unroll
       for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit32(dcur[v], g), m);
-      ntt_forward_regs<LOGN>(e, tid, T, ssm);
+      // Lazy outputs (below (1 + 2 LOGN) q < 2^40 for q < 2^35) feed the 96-bit sums directly.
+      ntt_forward_regs<LOGN, 0, true>(e, tid, T, ssm);
       const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * (p * L + L - 1 - k)) * n + 8 * tid);
       const ulonglong2* Kb = Km + n / 2;
 #pragma unroll
@@ -908,7 +910,7 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
 // CMux level o < count: fused kernel when the ring has one NTT limb of a
 // supported degree and a small gadget, else diff -> external product -> add.
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
-  return R.ntt && R.nl == 1 && g.small && g.S < ((u128)1 << 32) && R.m[0].q < (1ull << 40) &&
+  return R.ntt && R.nl == 1 && g.small && g.S < ((u128)1 << 32) && R.m[0].q < (1ull << 35) &&
          (R.n == 4096 || R.n == 2048 || R.n == 1024 || R.n == 512);
 }
 
