@@ -114,7 +114,7 @@ constexpr int NTT_THREADS = 256;
 // len and base = (u / stride) * (stride << r) + u % stride over the n >> r
 // sub-blocks u; a thread owns 8 >> r consecutive sub-blocks.
 // ---------------------------------------------------------------------------
-template <int LOGN, bool INV, int P>
+template <int LOGN, bool INV, int P, bool LAZY = false>
 __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* sm, int sbase,
                                            bool active) {
   using Ph = NttPhase<LOGN, INV, P>;
@@ -129,9 +129,11 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
   }
   Ph::run(e, tid, T);
   if constexpr (P == NPH - 1) {
+    if constexpr (INV || !LAZY) {
 #pragma unroll
-    for (int v = 0; v < 8; ++v)
-      e[v] = INV ? mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q) : ntt_canonical(e[v], T);
+      for (int v = 0; v < 8; ++v)
+        e[v] = INV ? mul_shoup(e[v], T.ninv[LOGN], T.ninv_sh[LOGN], T.q) : ntt_canonical(e[v], T);
+    }
     if (active) {
 #pragma unroll
       for (int v = 0; v < 8; ++v) g[Ph::index(v, tid)] = e[v];
@@ -140,7 +142,7 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) sm[swz(sbase + Ph::index(v, tid))] = e[v];
-    ntt_phases<LOGN, INV, P + 1>(e, tid, T, g, sm, sbase, active);
+    ntt_phases<LOGN, INV, P + 1, LAZY>(e, tid, T, g, sm, sbase, active);
   }
 }
 
@@ -150,7 +152,9 @@ __host__ __device__ constexpr int ntt_cta() {
   return ((1 << LOGN) / 8) > NTT_THREADS ? ((1 << LOGN) / 8) : NTT_THREADS;
 }
 
-template <int LOGN, bool INV>
+// LAZY (forward only): outputs left below (1 + 2 LOGN) q, for digit transforms
+// whose consumer reduces a 128-bit sum of products.
+template <int LOGN, bool INV, bool LAZY = false>
 __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg(u64* __restrict__ data, int nl, long segments,
                                                              NttTable t0, NttTable t1) {
   constexpr int n = 1 << LOGN;
@@ -163,7 +167,7 @@ __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg(u64* __restrict__ d
   const bool active = seg < segments;
   const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
   u64 e[8];
-  ntt_phases<LOGN, INV, 0>(e, tid, T, data + seg * n, sm, seg_local * n, active);
+  ntt_phases<LOGN, INV, 0, LAZY>(e, tid, T, data + seg * n, sm, seg_local * n, active);
 }
 
 // n = 2 and 4: one thread per segment, all in registers.
@@ -208,7 +212,7 @@ __global__ void k_ntt_tiny(u64* __restrict__ data, int nl, long segments, NttTab
   for (int i = 0; i < n; ++i) g[i] = a[i];
 }
 
-template <bool INV>
+template <bool INV, bool LAZY = false>
 static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
                    cudaStream_t st) {
   if (segments <= 0) return;
@@ -226,7 +230,7 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
   unsigned blocks = (unsigned)((segments + spc - 1) / spc);
   switch (logn) {
 #define VIA_NTT_CASE(LG) \
-  case LG: k_ntt_reg<LG, INV><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1); break;
+  case LG: k_ntt_reg<LG, INV, LAZY><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1); break;
     VIA_NTT_CASE(3)
     VIA_NTT_CASE(4)
     VIA_NTT_CASE(5)
@@ -247,6 +251,10 @@ void ntt_forward(u64* data, int n, int nl, long segments, const NttTable& t0, co
 }
 void ntt_inverse(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1, cudaStream_t st) {
   launch<true>(data, n, nl, segments, t0, t1, st);
+}
+void ntt_forward_lazy(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
+                      cudaStream_t st) {
+  launch<false, true>(data, n, nl, segments, t0, t1, st);
 }
 
 }  // namespace via

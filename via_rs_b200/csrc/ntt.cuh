@@ -186,5 +186,9 @@ void ntt_forward(u64* data, int n, int nl, long segments, const NttTable& t0, co
                  cudaStream_t st);
 void ntt_inverse(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
                  cudaStream_t st);
+// Forward transform whose outputs are left below (1 + 2 log2 n) q (n >= 8;
+// n = 2, 4 give exact residues), for operands of a 128-bit sum of products.
+void ntt_forward_lazy(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
+                      cudaStream_t st);
 
 }  // namespace via

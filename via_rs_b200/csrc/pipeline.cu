@@ -599,6 +599,12 @@ int workspace_batch(Server& s) { return s.ws ? s.ws->bmax : 0; }
 static void to_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
   if (R.ntt) ntt_forward(data, n, R.nl, segments, R.t[0], R.t[1], st);
 }
+// Eval form of gadget digits: the lazy forward transform (outputs below
+// (1 + 2 log2 n) q < 2^44 for q < 2^40, n <= 4096); their consumers add at most
+// a few dozen products with key residues below q into 128-bit sums.
+static void digits_to_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
+  if (R.ntt) ntt_forward_lazy(data, n, R.nl, segments, R.t[0], R.t[1], st);
+}
 static void from_eval(const DevRing& R, u64* data, int n, long segments, cudaStream_t st) {
   if (R.ntt) ntt_inverse(data, n, R.nl, segments, R.t[0], R.t[1], st);
 }
@@ -626,7 +632,7 @@ static void decompose(const DevRing& R, const Gadget& g, const u64* in, int n_in
 static void gadget_product(const DevRing& R, const Gadget& g, const u64* in, int n, int stride, int G, long nout,
                            KeySel ks, u64* out, u64* digits, cudaStream_t st) {
   decompose(R, g, in, n / stride, stride, (long)G * nout, digits, st);
-  to_eval(R, digits, n, (long)G * nout * g.L * R.nl, st);
+  digits_to_eval(R, digits, n, (long)G * nout * g.L * R.nl, st);
   mac(R, digits, ks, out, G * g.L, n, nout, st);
 }
 
@@ -667,7 +673,7 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
     if (R.ntt) {
       // Digits at the input degree; see k_cascade_mac for the repeated slots.
       decompose(R, w.g_ck, mi, n_in, 1, polys, digits, st);
-      if (n_in > 1) to_eval(R, digits, n_in, polys * L * nl, st);
+      if (n_in > 1) digits_to_eval(R, digits, n_in, polys * L * nl, st);
       int jj = std::min(rank_in / 2, 8), tt = std::min(n_out, 256 / jj);
       // Split the output masks over JB blocks while the grid is below ~4 blocks
       // per SM and every block keeps at least one mask per thread row.
