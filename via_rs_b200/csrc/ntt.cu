@@ -114,14 +114,24 @@ constexpr int NTT_THREADS = 256;
 // len and base = (u / stride) * (stride << r) + u % stride over the n >> r
 // sub-blocks u; a thread owns 8 >> r consecutive sub-blocks.
 // ---------------------------------------------------------------------------
-template <int LOGN, bool INV, int P, bool LAZY = false>
+// I8: the segment's input is a polynomial of signed 8-bit digits at `gin`,
+// lifted into [0, q) on load; the output goes to g.
+template <int LOGN, bool INV, int P, bool LAZY = false, bool I8 = false>
 __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable& T, u64* g, u64* sm, int sbase,
-                                           bool active) {
+                                           bool active, const int8_t* gin = nullptr) {
   using Ph = NttPhase<LOGN, INV, P>;
   constexpr int NPH = (LOGN + 2) / 3;
   if (P == 0) {
+    if constexpr (I8) {
 #pragma unroll
-    for (int v = 0; v < 8; ++v) e[v] = active ? g[Ph::index(v, tid)] : 0;
+      for (int v = 0; v < 8; ++v) {
+        const int d = active ? gin[Ph::index(v, tid)] : 0;
+        e[v] = d >= 0 ? (u64)d : T.q - (u64)(-d);
+      }
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = active ? g[Ph::index(v, tid)] : 0;
+    }
   } else {
     __syncthreads();
 #pragma unroll
@@ -142,7 +152,7 @@ __device__ __forceinline__ void ntt_phases(u64 (&e)[8], int tid, const NttTable&
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) sm[swz(sbase + Ph::index(v, tid))] = e[v];
-    ntt_phases<LOGN, INV, P + 1, LAZY>(e, tid, T, g, sm, sbase, active);
+    ntt_phases<LOGN, INV, P + 1, LAZY, false>(e, tid, T, g, sm, sbase, active);
   }
 }
 
@@ -168,6 +178,55 @@ __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg(u64* __restrict__ d
   const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
   u64 e[8];
   ntt_phases<LOGN, INV, 0, LAZY>(e, tid, T, data + seg * n, sm, seg_local * n, active);
+}
+
+// Lazy forward transforms of signed 8-bit digit polynomials: segment s (limb
+// s % nl of digit polynomial s / nl) reads din + (s / nl) * n and writes
+// out + s * n.
+template <int LOGN>
+__global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg_i8(const int8_t* __restrict__ din, u64* __restrict__ out,
+                                                                int nl, long segments, NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  constexpr int TPS = n / 8;
+  constexpr int SPC = ntt_cta<LOGN>() / TPS;
+  __shared__ u64 sm[ntt_cta<LOGN>() * 8];
+  const int seg_local = threadIdx.x / TPS;
+  const int tid = threadIdx.x % TPS;
+  const long seg = (long)blockIdx.x * SPC + seg_local;
+  const bool active = seg < segments;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  u64 e[8];
+  ntt_phases<LOGN, false, 0, true, true>(e, tid, T, out + seg * n, sm, seg_local * n, active,
+                                         din + (active ? seg / nl : 0) * n);
+}
+
+// n = 2 and 4 on 8-bit digits: one thread per segment.
+template <int LOGN>
+__global__ void k_ntt_tiny_i8(const int8_t* __restrict__ din, u64* __restrict__ out, int nl, long segments,
+                              NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  long seg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  const u64 q = T.q;
+  u64 a[n];
+  const int8_t* gi = din + (seg / nl) * n;
+#pragma unroll
+  for (int i = 0; i < n; ++i) a[i] = gi[i] >= 0 ? (u64)gi[i] : q - (u64)(-gi[i]);
+#pragma unroll
+  for (int len = n / 2, m = 1; len >= 1; len >>= 1, m <<= 1)
+#pragma unroll
+    for (int x = 0; x < n; ++x) {
+      if ((x / len) & 1) continue;
+      const int grp = x / (2 * len);
+      const u64 t = mul_shoup(a[x + len], T.psi[m + grp], T.psi_sh[m + grp], q);
+      const u64 u = a[x];
+      a[x] = addmod(u, t, q);
+      a[x + len] = submod(u, t, q);
+    }
+  u64* g = out + seg * n;
+#pragma unroll
+  for (int i = 0; i < n; ++i) g[i] = a[i];
 }
 
 // n = 2 and 4: one thread per segment, all in registers.
@@ -255,6 +314,39 @@ void ntt_inverse(u64* data, int n, int nl, long segments, const NttTable& t0, co
 void ntt_forward_lazy(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
                       cudaStream_t st) {
   launch<false, true>(data, n, nl, segments, t0, t1, st);
+}
+
+void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segments, const NttTable& t0,
+                         const NttTable& t1, cudaStream_t st) {
+  if (segments <= 0) return;
+  const int logn = __builtin_ctz((unsigned)n);
+  if (n < 2 || (n & (n - 1)) || logn > 12) throw CudaError(100, "ntt: degree must be a power of two in [2, 4096]");
+  if (logn <= 2) {
+    const unsigned blocks = (unsigned)((segments + 127) / 128);
+    if (logn == 1) k_ntt_tiny_i8<1><<<blocks, 128, 0, st>>>(din, out, nl, segments, t0, t1);
+    else k_ntt_tiny_i8<2><<<blocks, 128, 0, st>>>(din, out, nl, segments, t0, t1);
+    VIA_LAUNCHED();
+    return;
+  }
+  const int cta = std::max(NTT_THREADS, n / 8);
+  const long spc = cta / (n / 8);
+  const unsigned blocks = (unsigned)((segments + spc - 1) / spc);
+  switch (logn) {
+#define VIA_NTT_I8_CASE(LG) \
+  case LG: k_ntt_reg_i8<LG><<<blocks, cta, 0, st>>>(din, out, nl, segments, t0, t1); break;
+    VIA_NTT_I8_CASE(3)
+    VIA_NTT_I8_CASE(4)
+    VIA_NTT_I8_CASE(5)
+    VIA_NTT_I8_CASE(6)
+    VIA_NTT_I8_CASE(7)
+    VIA_NTT_I8_CASE(8)
+    VIA_NTT_I8_CASE(9)
+    VIA_NTT_I8_CASE(10)
+    VIA_NTT_I8_CASE(11)
+    VIA_NTT_I8_CASE(12)
+#undef VIA_NTT_I8_CASE
+  }
+  VIA_LAUNCHED();
 }
 
 }  // namespace via

@@ -190,5 +190,9 @@ void ntt_inverse(u64* data, int n, int nl, long segments, const NttTable& t0, co
 // n = 2, 4 give exact residues), for operands of a 128-bit sum of products.
 void ntt_forward_lazy(u64* data, int n, int nl, long segments, const NttTable& t0, const NttTable& t1,
                       cudaStream_t st);
+// The same from signed 8-bit digit polynomials: segment s (limb s % nl of
+// polynomial s / nl) reads din + (s / nl) * n and writes out + s * n.
+void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segments, const NttTable& t0,
+                         const NttTable& t1, cudaStream_t st);
 
 }  // namespace via

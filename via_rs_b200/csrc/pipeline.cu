@@ -54,6 +54,25 @@ __global__ void k_decompose(const u64* __restrict__ in, int n_in, int stride, lo
   });
 }
 
+// The same digits as signed bytes for gadgets with B <= 255 (|digit| <= 127),
+// limb-free: out [p][L][n_in] in sample order; the 8-bit transforms lift them
+// per limb. A sixteenth of the bytes of the u64 digits of a two-limb ring.
+__global__ void k_decompose_i8(const u64* __restrict__ in, int n_in, long npolys, DevRing R, Gadget g,
+                               int8_t* __restrict__ out) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= npolys * n_in) return;
+  const long p = gid / n_in;
+  const int i = (int)(gid % n_in);
+  const int nl = R.nl;
+  const u64* src = in + p * nl * n_in;
+  const u64 a0 = src[i], a1 = nl == 2 ? src[n_in + i] : 0;
+  int8_t* o = out + p * (long)g.L * n_in + (long)(g.L - 1) * n_in + i;
+  for_each_digit(gadget_scaled(a0, a1, R, g), g, [&](int, i64 d) {
+    *o = (int8_t)d;
+    o -= n_in;
+  });
+}
+
 // Which eval-form key samples output o multiplies: K_o = base + ((o / div) % mod) * stride.
 // stride = 0 means "consecutive keys" (T*2*nl*n residues apart, T = samples per key).
 struct KeySel {
@@ -448,6 +467,7 @@ struct Workspace {
   // Cascade.
   DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
   DevBuf c_bpart;  // k_cascade_mac body partials when the masks are split over blocks
+  DevBuf c_dig8;   // 8-bit cascade / conversion-key digits [lwe][n1 * L_CK] bytes (base <= 255)
   // RLWE -> RGSW.
   // RGSWs grouped by use: the DMux bits of every query ([q][nd]), then the
   // CMux and CRot bits ([q][nbits - nd]), each [2L][2][nl][n1] at q1.
@@ -529,6 +549,7 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   A(w->c_digits, nlwe * (s.r1.ntt ? 1 : 2) * n1 * Lck * nl);
   A(w->c_P, s.r1.ntt ? 0 : nlwe * 2 * n1 * 2 * nl);
   A(w->c_bsum, nlwe * n1 * nl);
+  A(w->c_dig8, p.ck_base <= 255 && s.r1.ntt ? (nlwe * n1 * Lck + 7) / 8 : 0);
   // A split grid has at most CASCADE_SPLIT_BLOCKS blocks of at most 256 slots.
   // Two halves: the answer's stream and the side stream expand concurrently.
   A(w->c_bpart, s.r1.ntt ? 2L * CASCADE_SPLIT_BLOCKS * 256 : 0);
@@ -663,6 +684,8 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
   u64* cP = R.ntt ? nullptr : w.c_P.p + lwe0 * 2 * n1 * 2 * nl;
   u64* bsum = w.c_bsum.p + lwe0 * lwe_n;
   u64* rlwe = w.c_rlwe.p + lwe0 * 2 * lwe_n;
+  // Bases up to 255: digits as bytes, lifted and transformed by the 8-bit NTT.
+  int8_t* dig8 = w.c_dig8.p ? reinterpret_cast<int8_t*>(w.c_dig8.p) + lwe0 * (long)n1 * L : nullptr;
   k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query + lwe0 * (long)lwe_len(p), n1, nl, nlwe, mi, bi);
   VIA_LAUNCHED();
   const u64 step_len = (u64)2 * n1 * L * 2 * nl;
@@ -672,8 +695,14 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
     const long polys = nlwe * rank_in;
     if (R.ntt) {
       // Digits at the input degree; see k_cascade_mac for the repeated slots.
-      decompose(R, w.g_ck, mi, n_in, 1, polys, digits, st);
-      if (n_in > 1) digits_to_eval(R, digits, n_in, polys * L * nl, st);
+      if (dig8 && n_in > 1) {
+        k_decompose_i8<<<blocks(polys * n_in, 128), 128, 0, st>>>(mi, n_in, polys, R, w.g_ck, dig8);
+        VIA_LAUNCHED();
+        ntt_forward_i8_lazy(dig8, digits, n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
+      } else {
+        decompose(R, w.g_ck, mi, n_in, 1, polys, digits, st);
+        if (n_in > 1) digits_to_eval(R, digits, n_in, polys * L * nl, st);
+      }
       int jj = std::min(rank_in / 2, 8), tt = std::min(n_out, 256 / jj);
       // Split the output masks over JB blocks while the grid is below ~4 blocks
       // per SM and every block keeps at least one mask per thread row.
@@ -708,7 +737,15 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
   // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178); the
   // final rank-1 masks are already contiguous [lwe][nl][n1] in `mi`.
   u64* gp = w.g_gp.p + lwe0 * 2 * lwe_n;
-  gadget_product(R, w.g_ck, mi, n1, 1, 1, nlwe, keys_shared(s.conv_eval.p), gp, w.g_digits.p + lwe0 * L * lwe_n, st);
+  u64* gdig = w.g_digits.p + lwe0 * L * lwe_n;
+  if (dig8) {
+    k_decompose_i8<<<blocks(nlwe * n1, 128), 128, 0, st>>>(mi, n1, nlwe, R, w.g_ck, dig8);
+    VIA_LAUNCHED();
+    ntt_forward_i8_lazy(dig8, gdig, n1, nl, nlwe * L * nl, R.t[0], R.t[1], st);
+    mac(R, gdig, keys_shared(s.conv_eval.p), gp, L, n1, nlwe, st);
+  } else {
+    gadget_product(R, w.g_ck, mi, n1, 1, 1, nlwe, keys_shared(s.conv_eval.p), gp, gdig, st);
+  }
   from_eval(R, gp, n1, nlwe * 2 * nl, st);
   k_assemble_rgsw<<<blocks(nlwe * 2 * nl * n1), 256, 0, st>>>(rlwe, gp, (int)p.l_query, nbits, n1, nl, R,
                                                                w.rgsw_q1.p + bit0 * rgsw1);
