@@ -177,11 +177,13 @@ __global__ void k_rlwe_addsub(u64* out, const u64* a, long sa, const u64* b, lon
 }
 
 // The trivial RLWE (0, delta) at q1 (answer.rs:181-191): zero mask, body = delta * X^0.
-__global__ void k_set_trivial(u64* ct, int n, int nl, u64 d0, u64 d1) {
-  int gid = blockIdx.x * blockDim.x + threadIdx.x;
-  if (gid >= 2 * nl * n) return;
-  int poly = gid / (nl * n), rem = gid % (nl * n);
-  int l = rem / n, i = rem % n;
+// `count` trivial RLWEs (0, d) with d the constant (d0, d1) in RNS form.
+__global__ void k_set_trivial(u64* ct, long count, int n, int nl, u64 d0, u64 d1) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid >= count * 2 * nl * n) return;
+  const long r = gid % (2L * nl * n);
+  const int poly = (int)(r / (nl * n)), rem = (int)(r % (nl * n));
+  const int l = rem / n, i = rem % n;
   ct[gid] = (poly == 1 && i == 0) ? (l == 0 ? d0 : d1) : 0;
 }
 
@@ -1123,11 +1125,9 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   {
     u128 Q1 = s.r1.Q();
     u128 delta = (Q1 + p.p - 1) / p.p;
-    for (long q = 0; q < B; ++q) {
-      k_set_trivial<<<blocks(2 * nl * n1), 256, 0, st>>>(w.dm_a.p + q * 2 * nl * n1, n1, nl,
-                                                         (u64)(delta % s.r1.m[0].q), (u64)(delta % s.r1.m[1].q));
-      VIA_LAUNCHED();
-    }
+    k_set_trivial<<<blocks(B * 2 * nl * n1), 256, 0, st>>>(w.dm_a.p, B, n1, nl, (u64)(delta % s.r1.m[0].q),
+                                                           (u64)(delta % s.r1.m[1].q));
+    VIA_LAUNCHED();
     u64 *in = w.dm_a.p, *out = w.dm_b.p;
     for (int i = 0; i < nd; ++i) {
       const long active = 1L << i;  // per query
