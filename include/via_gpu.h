@@ -188,6 +188,17 @@ via_status via_first_dim_dev(via_server* s, const uint64_t* switched, uint64_t* 
 via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
 
 /*
+ * The server's own negacyclic transform at (q2, n1), in place on `count`
+ * polynomials of n1 residues: forward (inverse = 0) gives the eval form the
+ * scan entry points above take and return, inverse (inverse = 1) brings their
+ * outputs back to coefficients. The order of eval slots is this library's
+ * (first_dim.rs:94-184 only observes coefficient-form results). Servers whose
+ * q2 has no NTT use coefficients as their eval form: the call is a no-op.
+ * Enqueued on `stream`.
+ */
+via_status via_server_transform_q2_dev(via_server* s, uint64_t* data, uint64_t count, int inverse, void* stream);
+
+/*
  * The scans of n_queries independent queries in one pass over the database
  * (the T first_dim calls of answer_batch, srv/batch.rs:139-150, sharing the
  * scan): `sel_eval` holds [n_queries][I][2][n1] eval-form selection RLWEs,
@@ -355,16 +366,21 @@ via_status via_server_answer_wire(via_server* s, const uint8_t* wire, uint64_t l
 
 /*
  * The FirstDim scan of via_first_dim_scan_dev for callers that cannot allocate
- * device memory: code that runs where cudaMalloc is not allowed or not wanted
- * (inside a region being captured into a CUDA graph, a host whose allocator is
- * owned by another runtime, a latency-critical path that must not hit the
- * allocator). It allocates nothing: its scratch (the split selection vectors)
- * is a static 8 MiB device array that the library holds on every device until
- * exit, so it requires num_rows * 2 * n1 <= 2^20 (I <= 256 at n1 = 2048) and
- * returns VIA_ERR_INVALID_ARGUMENT above that. The first call on a device looks
- * up the array's device address; make it before any stream capture. Calls that
- * overlap on the GPU race on the shared array. This entry point has no
- * counterpart in the reference.
+ * device memory: a host whose device memory is owned by another runtime's
+ * allocator or a fixed pool (cudaMalloc there would fail or bypass its
+ * accounting), or a latency-critical path that must not enter the allocator,
+ * which can synchronize the device. It allocates nothing: its scratch (the
+ * split selection vectors) is a static 8 MiB device array that the library
+ * holds on every device until exit. It requires 16 * I_pad * n1 <= 2^23 bytes,
+ * I_pad = num_rows rounded up to 64 (I <= 256 at n1 = 2048, I <= 128 at
+ * n1 = 4096), and returns VIA_ERR_INVALID_ARGUMENT above that; servers whose
+ * q2 has no NTT (schoolbook rings) use no scratch and have no limit. Call it
+ * with the server's device current (else VIA_ERR_INVALID_ARGUMENT). The first
+ * call on a device looks up the array's device address; make it before any
+ * stream capture. Calls share the array, which keeps the last call's contents:
+ * calls whose work overlaps on the GPU race on it. Like via_first_dim_scan_dev
+ * it returns once the scan is enqueued. This entry point has no counterpart in
+ * the reference.
  */
 via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream);
 

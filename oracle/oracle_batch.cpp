@@ -7,6 +7,10 @@
 //   crates/via-primitives/src/conversion/repack.rs:650-739     q1 -> q2 key derivation
 //   crates/via-server/src/batch.rs:72-163                      answer_batch
 //   crates/via-client/src/batch.rs:35-58                       deinterleave_batch
+#include <exception>
+#include <mutex>
+#include <thread>
+
 #include "via_oracle.hpp"
 
 namespace vo {
@@ -116,8 +120,32 @@ void answer_batch(const Params& prm, const std::vector<std::vector<Lwe>>& querie
                   Poly& body_q4) {
   const size_t T = (size_t)(prm.n2 / prm.n_rec);
   if (queries.size() != T) throw OracleError(ERR_DIM_MISMATCH, "answer_batch: batch.len() must equal T");
-  std::vector<Rlwe> rotated;
-  for (const auto& q : queries) rotated.push_back(answer_through_crot(prm, q, k, db, threads));
+  // The reference runs the T prefixes one after another (batch.rs:134-145).
+  // They are independent, so the checker spreads them over its threads (each
+  // prefix then scans single-threaded); the results are the same.
+  std::vector<Rlwe> rotated(T);
+  if (threads > 1 && T > 1) {
+    const size_t w = std::min((size_t)threads, T);
+    std::exception_ptr err;
+    std::mutex mu;
+    std::vector<std::thread> ts;
+    for (size_t t = 0; t < w; ++t)
+      ts.emplace_back([&, t] {
+        for (size_t i = t; i < T; i += w) {
+          try {
+            rotated[i] = answer_through_crot(prm, queries[i], k, db, 1);
+          } catch (...) {
+            std::lock_guard<std::mutex> g(mu);
+            if (!err) err = std::current_exception();
+            return;
+          }
+        }
+      });
+    for (auto& th : ts) th.join();
+    if (err) std::rethrow_exception(err);
+  } else {
+    for (size_t i = 0; i < T; ++i) rotated[i] = answer_through_crot(prm, queries[i], k, db, threads);
+  }
   Rlwe packed = repack(prm, rotated, rkeys);
   resp_comp(prm, packed, k.rsk, mask_q3, body_q4);
 }

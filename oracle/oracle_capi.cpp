@@ -190,8 +190,10 @@ void vo_client_secret(void* c, uint64_t* sk1, uint64_t* sk2) {
 void vo_client_free(void* c) { delete (Client*)c; }
 
 // Server::setup (srv/answer.rs:486-528). Records: n_rec u64 coefficients each.
-void* vo_server_setup(const via_params* p, const uint64_t* cascade, const uint64_t* conv, const uint64_t* rsk,
-                      const uint64_t* records, size_t n_records, int threads) {
+// records: u64 coefficients (packed == 0) or 4-bit coefficients two per byte,
+// low nibble first (packed == 1).
+static void* server_setup(const via_params* p, const uint64_t* cascade, const uint64_t* conv, const uint64_t* rsk,
+                          const void* records, int packed, size_t n_records, int threads) {
   OracleServer* out = nullptr;
   guarded([&] {
     auto s = std::make_unique<OracleServer>();
@@ -207,10 +209,21 @@ void* vo_server_setup(const via_params* p, const uint64_t* cascade, const uint64
     for (int j = 0; j < prm.d(); ++j) pk.rsk.push_back(get_rlev(src, R3, prm.l_rsk));
     s->keys = prepare_keys(prm, pk);
     s->cascade = pk.cascade;
-    s->db = setup_db(prm, records, n_records, threads);
+    s->db = packed ? setup_db_packed(prm, (const uint8_t*)records, n_records, threads)
+                   : setup_db(prm, (const u64*)records, n_records, threads);
     out = s.release();
   });
   return out;
+}
+
+void* vo_server_setup(const via_params* p, const uint64_t* cascade, const uint64_t* conv, const uint64_t* rsk,
+                      const uint64_t* records, size_t n_records, int threads) {
+  return server_setup(p, cascade, conv, rsk, records, 0, n_records, threads);
+}
+
+void* vo_server_setup_packed(const via_params* p, const uint64_t* cascade, const uint64_t* conv, const uint64_t* rsk,
+                             const uint8_t* packed, size_t n_records, int threads) {
+  return server_setup(p, cascade, conv, rsk, packed, 1, n_records, threads);
 }
 
 int vo_server_answer(void* sv, const uint64_t* query, size_t n_lwe, uint64_t* mask, uint64_t* body, int threads) {

@@ -582,7 +582,10 @@ static void parallel_for(size_t n, int threads, F f) {
   for (auto& t : ts) t.join();
 }
 
-PreparedDb setup_db(const Params& prm, const u64* records, size_t n_records, int threads) {
+// Record r's coefficient c: records[r * n_rec + c] (u64 layout) or the nibble
+// r * n_rec + c of `packed`, low nibble first (the 4-bit packed layout).
+template <class Coef>
+static PreparedDb setup_db_impl(const Params& prm, Coef coef, size_t n_records, int threads) {
   u64 I = prm.num_rows, J = prm.num_cols;
   int d = prm.n1 / prm.n_rec;
   if (n_records > I * J * (u64)d)
@@ -598,12 +601,21 @@ PreparedDb setup_db(const Params& prm, const u64* records, size_t n_records, int
     for (int k = 0; k < d; ++k) {
       u64 flat = (u64)k * I * J + i * J + j;
       if (flat >= n_records) continue;
-      const u64* rec = records + flat * prm.n_rec;
-      for (int c = 0; c < prm.n_rec; ++c) v[(size_t)d * c + k] = (v[(size_t)d * c + k] + rec[c]) % prm.p;
+      for (int c = 0; c < prm.n_rec; ++c)
+        v[(size_t)d * c + k] = (v[(size_t)d * c + k] + coef(flat * prm.n_rec + c)) % prm.p;
     }
     db.cells[cell] = R2.to_eval(R2.from_u128(v));
   });
   return db;
+}
+
+PreparedDb setup_db(const Params& prm, const u64* records, size_t n_records, int threads) {
+  return setup_db_impl(prm, [records](u64 x) { return records[x]; }, n_records, threads);
+}
+
+PreparedDb setup_db_packed(const Params& prm, const uint8_t* packed, size_t n_records, int threads) {
+  return setup_db_impl(
+      prm, [packed](u64 x) { return (u64)((packed[x >> 1] >> (4 * (x & 1))) & 15); }, n_records, threads);
 }
 
 std::vector<Rlwe> first_dim(const Params& prm, const std::vector<Rlwe>& switched, const PreparedDb& db, int threads) {

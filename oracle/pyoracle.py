@@ -43,6 +43,9 @@ def lib() -> ctypes.CDLL:
         L.vo_client_secret.argtypes = [ctypes.c_void_p, _u64p, _u64p]
         L.vo_server_setup.restype = ctypes.c_void_p
         L.vo_server_setup.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p, _u64p, ctypes.c_size_t, ctypes.c_int]
+        L.vo_server_setup_packed.restype = ctypes.c_void_p
+        L.vo_server_setup_packed.argtypes = [ctypes.c_void_p, _u64p, _u64p, _u64p, ctypes.c_void_p, ctypes.c_size_t,
+                                             ctypes.c_int]
         L.vo_server_answer.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, _u64p, _u64p, ctypes.c_int]
         L.vo_server_answer_batch.argtypes = [ctypes.c_void_p, _u64p, ctypes.c_size_t, ctypes.c_size_t, _u64p, _u64p,
                                              ctypes.c_int]
@@ -205,13 +208,21 @@ class Server:
     """Server::setup / answer on the CPU (crates/via-server/src/answer.rs)."""
 
     def __init__(self, prm: Params, cascade_key, conv_key, rsk, records: np.ndarray, threads: int = 0):
+        """records: u64 coefficients [n_records][n_rec], or a uint8 array of 4-bit
+        coefficients packed two per byte, low nibble first (n_records * n_rec / 2 bytes)."""
         self.prm = prm
         self.threads = threads or os.cpu_count() or 1
         self._cp = prm.to_c()
-        rec = np.ascontiguousarray(records, dtype=np.uint64)
-        n_rec = rec.size // prm.n_rec
-        h = lib().vo_server_setup(ctypes.byref(self._cp), _ptr(cascade_key), _ptr(conv_key), _ptr(rsk),
-                                  _ptr(rec), n_rec, self.threads)
+        if records.dtype == np.uint8:
+            rec = np.ascontiguousarray(records).reshape(-1)
+            n_rec = rec.size * 2 // prm.n_rec
+            h = lib().vo_server_setup_packed(ctypes.byref(self._cp), _ptr(cascade_key), _ptr(conv_key), _ptr(rsk),
+                                             rec.ctypes.data_as(ctypes.c_void_p), n_rec, self.threads)
+        else:
+            rec = np.ascontiguousarray(records, dtype=np.uint64)
+            n_rec = rec.size // prm.n_rec
+            h = lib().vo_server_setup(ctypes.byref(self._cp), _ptr(cascade_key), _ptr(conv_key), _ptr(rsk),
+                                      _ptr(rec), n_rec, self.threads)
         if not h:
             raise OracleError(-1, lib().vo_last_error().decode())
         self._h = h

@@ -309,6 +309,8 @@ struct PreparedDb {
 // setup_db (srv/setup_db.rs:39-75) + PreparedDb::from_encoded (srv/prepared_db.rs:57-85).
 // records: n_records polynomials of degree n_rec, coefficients in [0, p).
 PreparedDb setup_db(const Params& prm, const u64* records, size_t n_records, int threads);
+// The same from 4-bit records packed two per byte, low nibble first.
+PreparedDb setup_db_packed(const Params& prm, const uint8_t* packed, size_t n_records, int threads);
 // srv/first_dim.rs:94-184; threads > 1 fans the J loop like the reference.
 std::vector<Rlwe> first_dim(const Params& prm, const std::vector<Rlwe>& switched, const PreparedDb& db,
                             int threads);

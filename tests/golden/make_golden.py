@@ -58,7 +58,9 @@ def extract(text: str) -> dict:
 
 
 def main() -> None:
-    ref = pathlib.Path(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        raise SystemExit("usage: python tests/golden/make_golden.py <path of the via-rs checkout>")
+    ref = pathlib.Path(sys.argv[1])
     golden = {}
     for group, rel in FILES.items():
         golden[group] = extract((ref / rel).read_text())

@@ -47,18 +47,27 @@ def test_answer_batch_rejects_wrong_sizes(oracle):
         gpu.answer_batch(qs[:, : -prm.lwe_len])
 
 
-def test_answer_batch_t256_recovers(oracle):
-    """The production VIA-B batch: T = 256 records of degree 2 per answer (depth-10
-    repack). The oracle would take minutes for 256 queries, so the check is the
-    reference's e2e property: recover_batch returns every queried record."""
-    prm = paper_preset(2, 2, n_rec=2)
-    assert prm.n2 // prm.n_rec == 256
-    rng = np.random.default_rng(256)
+@pytest.mark.parametrize("T", [2, 4, 16, 32, 64, 128, 256])
+def test_answer_batch_every_t_matches_oracle(oracle, T):
+    """Every power-of-two batch size T = n2 / n_rec, records of degree n2 / T (the
+    reference's repack engine is generic over T, repack.rs:331-397; its record-fit
+    rule admits any power of two with T * n_rec <= n2, presets.rs:170-176). The
+    answer equals the oracle's and recover_batch returns every queried record.
+    T = 256 (records of degree 2) is the production VIA-B batch: a depth-10 repack."""
+    prm = paper_preset(2, 2, n_rec=512 // T)
+    assert prm.n2 // prm.n_rec == T
+    rng = np.random.default_rng(1000 + T)
     recs = rng.integers(0, 16, size=(prm.capacity, prm.n_rec), dtype=np.uint64)
-    client = oracle.Client(prm, b"gpu-via-b-t256")
+    client = oracle.Client(prm, b"gpu-via-b-t%d" % T)
     gpu = Server.setup(prm, PublicKeys(client.cascade_key, client.conv_key, client.rsk), recs)
-    idx = [int(i) for i in rng.integers(prm.capacity, size=256)]
-    gm, gb = gpu.answer_batch(client.batch_query(idx, b"t256"))
+    cpu = oracle.Server(prm, client.cascade_key, client.conv_key, client.rsk, recs)
+    idx = [int(i) for i in rng.integers(prm.capacity, size=T)]
+    qs = client.batch_query(idx, b"t%d" % T)
+    gm, gb = gpu.answer_batch(qs)
+    cm, cb = cpu.answer_batch(qs)
+    assert np.array_equal(gm, cm), f"T={T}: batch answer mask differs from the oracle"
+    assert np.array_equal(gb, cb), f"T={T}: batch answer body differs from the oracle"
     got = client.recover_batch(gm, gb)
     bad = [t for t, i in enumerate(idx) if not np.array_equal(got[t], recs[i])]
-    assert not bad, f"{len(bad)} of 256 records wrong, first slots {bad[:8]}"
+    assert not bad, f"T={T}: {len(bad)} records wrong, first slots {bad[:8]}"
+    gpu.close()

@@ -106,6 +106,9 @@ def lib() -> ctypes.CDLL:
                                              ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_server_reserve.restype = ctypes.c_int
     L.via_server_reserve.argtypes = [ctypes.c_void_p, ctypes.c_uint64]
+    L.via_server_transform_q2_dev.restype = ctypes.c_int
+    L.via_server_transform_q2_dev.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_uint64, ctypes.c_int,
+                                              ctypes.c_void_p]
     L.via_first_dim_scan_static.restype = ctypes.c_int
     L.via_first_dim_scan_static.argtypes = [ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     L.via_server_autotune.restype = ctypes.c_int

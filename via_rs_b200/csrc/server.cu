@@ -22,7 +22,8 @@ static thread_local std::string g_last_error;
 // byte planes padded to 16 rows per query and row, 16 * I * n1 bytes) live in
 // this file-scope device array instead of memory the call allocates. Every
 // device that loads the library holds it (8 MiB) until exit.
-constexpr u64 STATIC_SCAN_SCRATCH = 8ull << 20;  // bytes: 16 * I * n1 <= 2^23, i.e. I * 2 * n1 <= 2^20
+// bytes: 16 * I_pad * n1 <= 2^23 with I_pad = num_rows rounded up to 64 (I_pad <= 256 at n1 = 2048)
+constexpr u64 STATIC_SCAN_SCRATCH = 8ull << 20;
 static __device__ __align__(256) uint4 g_scan_scratch[STATIC_SCAN_SCRATCH / 16];
 // Device address of g_scan_scratch per device, resolved once with that device current.
 static std::mutex g_scan_scratch_mu;
@@ -410,6 +411,19 @@ via_status via_first_dim_scan_dev(via_server* s, const uint64_t* sel_eval, uint6
   });
 }
 
+via_status via_server_transform_q2_dev(via_server* s, uint64_t* data, uint64_t count, int inverse, void* stream) {
+  return guarded([&] {
+    if (!s || (!data && count)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
+    if (count > (1ull << 31)) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "too many polynomials");
+    if (!s->r2.ntt || count == 0) return;
+    cudaStream_t st = (cudaStream_t)stream;
+    if (inverse)
+      ntt_inverse(data, s->prm.n1, 1, (long)count, s->r2.t[0], s->r2.t[0], st);
+    else
+      ntt_forward(data, s->prm.n1, 1, (long)count, s->r2.t[0], s->r2.t[0], st);
+  });
+}
+
 via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, uint64_t n_queries,
                                        uint64_t* out_eval, void* stream) {
   return guarded([&] {
@@ -432,18 +446,25 @@ via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, 
 // whose work overlaps on the GPU race on it. Each call writes every scratch byte
 // that reaches its result (the padding rows it leaves alone only feed
 // accumulator columns that are never read), so nothing has to start at zero.
+// Like via_first_dim_scan_dev it returns once the scan is enqueued, so a scan
+// whose bounded waits ran out is reported by the handle's next synchronous call.
 via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, uint64_t* out_eval, void* stream) {
   return guarded([&] {
     if (!s || !sel_eval || !out_eval) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null argument");
-    const via_params& p = s->prm;
     const u64 need = s->tensor_fd() ? fd_sel_bytes(s->fd, 1) : 0;
     if (need > STATIC_SCAN_SCRATCH)
       throw ApiError(VIA_ERR_INVALID_ARGUMENT, "via_first_dim_scan_static: the split selection needs " +
-                                                   std::to_string(need) + " bytes (16 * num_rows * n1), more than the "
-                                                   "static scratch of " + std::to_string(STATIC_SCAN_SCRATCH) + " bytes");
+                                                   std::to_string(need) + " bytes (16 * I_pad * n1, I_pad = num_rows "
+                                                   "rounded up to 64), more than the static scratch of " +
+                                                   std::to_string(STATIC_SCAN_SCRATCH) + " bytes");
     int dev = 0;
     VIA_CUDA(cudaGetDevice(&dev));
+    if (dev != s->device)
+      throw ApiError(VIA_ERR_INVALID_ARGUMENT, "via_first_dim_scan_static: the current device (" +
+                                                   std::to_string(dev) + ") is not the server's device (" +
+                                                   std::to_string(s->device) + ")");
     if (dev < 0 || dev >= 128) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "device ordinal out of range");
+    std::lock_guard<std::mutex> g(s->mu);  // fd.tuned may be re-sorted by the autotuner
     uint8_t* scratch = nullptr;
     {
       std::lock_guard<std::mutex> g(g_scan_scratch_mu);
@@ -456,7 +477,6 @@ via_status via_first_dim_scan_static(via_server* s, const uint64_t* sel_eval, ui
       }
       scratch = g_scan_scratch_addr[dev];
     }
-    (void)p;
     first_dim_queries(*s, sel_eval, out_eval, 1, scratch, (cudaStream_t)stream);
   });
 }

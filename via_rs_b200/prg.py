@@ -54,6 +54,16 @@ class Shake256Prg:
                 return v
 
 
+def stream_bytes(seed: bytes, n: int) -> bytes:
+    """The first n bytes of Shake256Prg(seed), computed block by block in one
+    pass (the same bytes as Shake256Prg(seed).bytes(n), faster for large n)."""
+    if len(seed) > 64:
+        raise ValueError("seed longer than 64 bytes")
+    blocks = (n + BLOCK - 1) // BLOCK
+    h = hashlib.shake_256
+    return b"".join([h(seed + i.to_bytes(8, "little")).digest(BLOCK) for i in range(blocks)])[:n]
+
+
 def nibble_records(prg: Shake256Prg, n_records: int, n_rec: int) -> np.ndarray:
     """n_records records of n_rec 4-bit coefficients from the byte stream, two
     coefficients per byte, low nibble first. Returns uint64 coefficients."""

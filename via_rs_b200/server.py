@@ -194,6 +194,12 @@ class Server:
         check(_lib.lib().via_first_dim_scan_dev(self._h, ctypes.c_void_p(sel_eval_ptr), ctypes.c_void_p(out_eval_ptr),
                                                 ctypes.c_void_p(stream)))
 
+    def transform_q2_dev(self, data_ptr: int, count: int, inverse: bool = False, stream: int = 0) -> None:
+        """The server's own transform at (q2, n1), in place on `count` polynomials:
+        the eval form scan_dev / scan_many_dev take and return."""
+        check(_lib.lib().via_server_transform_q2_dev(self._h, ctypes.c_void_p(data_ptr), count, 1 if inverse else 0,
+                                                     ctypes.c_void_p(stream)))
+
     def scan_many_dev(self, sel_eval_ptr: int, n_queries: int, out_eval_ptr: int, stream: int = 0) -> None:
         """The scans of n_queries queries in one pass over the database (eval form)."""
         check(_lib.lib().via_first_dim_scan_many_dev(self._h, ctypes.c_void_p(sel_eval_ptr), n_queries,
