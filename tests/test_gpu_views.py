@@ -8,7 +8,7 @@ import time
 import numpy as np
 import pytest
 
-from via_rs_b200.mixed import MixedService, poisson_mix, via_b_route
+from via_rs_b200.mixed import POW2_BATCH_SIZES, MixedService, poisson_mix, via_b_route
 from via_rs_b200.params import paper_preset
 from via_rs_b200.server import PublicKeys, Server
 
@@ -109,13 +109,14 @@ def test_t256_batch_in_chunks_through_service(oracle):
 
 def test_mixed_poisson_stream(oracle):
     """Seeded Poisson arrivals of VIA-C queries and VIA-B requests of 1..256
-    indices (log-uniform), padded to T = 8 or 256; every answer equals the
-    answer given alone and recovers the requested records."""
+    indices (log-uniform), each padded to the smallest power-of-two batch size
+    T >= m; every answer equals the answer given alone and recovers the
+    requested records."""
     prm, recs, keys, base = _base(oracle, 4, 8, 34)
     cells = _cells(prm, recs)
     clients = {"c": oracle.Client(prm, b"views-34")}
     records = {"c": recs}
-    for t in (8, 256):
+    for t in POW2_BATCH_SIZES:
         pv = prm.with_dims(prm.num_rows, prm.num_cols, prm.n2 // t)
         clients[t] = oracle.Client(pv, b"views-34")
         records[t] = _view_records(pv, cells)
@@ -123,7 +124,7 @@ def test_mixed_poisson_stream(oracle):
     try:
         rng = np.random.default_rng(35)
         plan = []
-        for k, (gap, kind, m) in enumerate(poisson_mix(10, 40.0, seed=36)):
+        for k, (gap, kind, m) in enumerate(poisson_mix(14, 40.0, seed=36)):
             if kind == "c":
                 i = int(rng.integers(prm.capacity))
                 plan.append((gap, "c", [i], 1, clients["c"].query(i, b"mix-%d" % k)))
