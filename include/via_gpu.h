@@ -249,6 +249,19 @@ via_status via_server_set_scan_tile(via_server* s, uint32_t batch, const via_sca
 uint64_t via_scan_tile_candidates(via_server* s, uint32_t batch, via_scan_tile* out, uint64_t cap);
 
 /*
+ * Test hook for the scan's bounded device waits. With wait_us > 0 (at most
+ * 100000), every later FirstDim scan on this handle first makes its epilogue
+ * wait on a barrier that nothing completes, for wait_us microseconds; the wait
+ * runs out, the CTAs abort (after their copies and MMAs in flight have landed)
+ * and set the handle's error word, so the synchronous calls and service
+ * requests report VIA_ERR_TIMEOUT, as after a real stall. wait_us = 0 turns the
+ * hook off and clears the error word. Returns VIA_ERR_INVALID_ARGUMENT for
+ * servers on non-NTT rings (their scan has no waits). The reference has no
+ * device and no counterpart; its error contract is proto/error.rs:20-64.
+ */
+via_status via_server_set_scan_fault(via_server* s, uint32_t wait_us);
+
+/*
  * Runs the answer up to `stage` and copies that stage's output, in coefficient
  * form, to the host buffer `out` (for stage-by-stage parity checks):
  *   1 cascade RLWEs [n_lwe][2][nl][n1]      (query_decomp.rs:76-78)

@@ -116,6 +116,8 @@ def lib() -> ctypes.CDLL:
                                       ctypes.c_char_p, ctypes.POINTER(ScanTuning)]
     L.via_server_set_scan_tile.restype = ctypes.c_int
     L.via_server_set_scan_tile.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ScanTile)]
+    L.via_server_set_scan_fault.restype = ctypes.c_int
+    L.via_server_set_scan_fault.argtypes = [ctypes.c_void_p, ctypes.c_uint32]
     L.via_scan_tile_candidates.restype = ctypes.c_uint64
     L.via_scan_tile_candidates.argtypes = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ScanTile),
                                            ctypes.c_uint64]

@@ -38,6 +38,7 @@ struct KParams {
   int* err;
   int n, J, n_jt, n_kc, n_ct, N, Np, nq;
   int stages, grouped, acc_stride, nacc, tmem_cols, order;
+  unsigned fault_ns;  // test hook: > 0 makes the epilogue's first wait run out after this long
   DevMod m;
 };
 
@@ -80,6 +81,17 @@ __device__ bool mbar_wait(u64* bar, u32 parity, volatile int* abort_flag, bool h
       if (honor_abort && *abort_flag) return false;
       if (global_ns() - t0 > WAIT_NS) return false;
     }
+  }
+  return false;
+}
+
+// The test hook's wait: polls a barrier that no thread or copy ever completes
+// until `limit_ns` has passed (or WAIT_SPINS polls), then reports failure.
+__device__ bool mbar_wait_never(u64* bar, unsigned limit_ns) {
+  const unsigned long long t0 = global_ns();
+  for (unsigned it = 0; it < WAIT_SPINS; ++it) {
+    if (mbar_try_wait(bar, 0)) return true;
+    if ((it & 31) == 0 && global_ns() - t0 > limit_ns) return false;
   }
   return false;
 }
@@ -170,7 +182,8 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
   u64* acc_full = empty + P.stages;
   u64* acc_empty = acc_full + 2;
   u64* drain = acc_empty + 2;
-  u32* tmem_slot = reinterpret_cast<u32*>(drain + 1);
+  u64* never = drain + 1;  // the test hook's barrier: initialised, never arrived on
+  u32* tmem_slot = reinterpret_cast<u32*>(never + 1);
   volatile int* abort_flag = reinterpret_cast<volatile int*>(tmem_slot + 1);
 
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -184,6 +197,7 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
       mbar_init(acc_empty + a, EPI_WARPS * 32);
     }
     mbar_init(drain, 1);
+    mbar_init(never, 1);
     *abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
   }
@@ -310,7 +324,8 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
     const int row = quad * 32 + lane;
     int a = 0;
     u32 aph = 0;
-    bool ok = true;
+    // The test hook: a wait that runs out before any accumulator is read.
+    bool ok = P.fault_ns == 0 || mbar_wait_never(never, P.fault_ns);
     for (int u = blockIdx.x; ok && u < units; u += gridDim.x) {
       int t, ct;
       unit_coords(P, u, t, ct);
@@ -609,6 +624,7 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
   K.nacc = T.nacc;
   K.tmem_cols = T.tmem_cols;
   K.order = T.order;
+  K.fault_ns = p.fault_wait_ns;
   K.m = p.m;
   const int units = p.n * T.n_ct;
   const int grid = std::min(units, p.grid);

@@ -50,6 +50,10 @@ struct FdPlan {
   int grid = 148;          // persistent CTAs (one per SM)
   int smem_max = 0;        // opt-in shared memory per block on this device
   int* err = nullptr;      // device word: nonzero after a bounded wait ran out
+  // Test hook (via_server_set_scan_fault): when nonzero, the epilogue of every
+  // CTA first waits on a barrier that nothing completes, bounded by this many
+  // nanoseconds, so the scan's abort path runs and the error word is set.
+  unsigned fault_wait_ns = 0;
   // Tuned tiles by batch size, sorted by batch. A scan of nq queries uses the
   // entry of the smallest tuned batch >= nq of the same kind (one query or a
   // batch), else the largest below it, else the default.

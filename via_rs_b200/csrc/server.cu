@@ -644,6 +644,7 @@ via_status via_server_set_scan_tile(via_server* s, uint32_t batch, const via_sca
   return guarded([&] {
     if (!s || batch == 0 || batch > 4096) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null handle or bad batch size");
     std::lock_guard<std::mutex> g(s->mu);
+    std::unique_lock<std::shared_mutex> plan(s->plan_mu);  // service workers read fd.tuned under plan_mu
     if (!s->tensor_fd()) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "this server's scan has no tiles (schoolbook ring)");
     if (!tile) {
       auto& v = s->fd.tuned;
@@ -655,6 +656,23 @@ via_status via_server_set_scan_tile(via_server* s, uint32_t batch, const via_sca
       fd_set_tile(s->fd, (int)batch, t);
     }
     ++s->plan_gen;
+  });
+}
+
+via_status via_server_set_scan_fault(via_server* s, uint32_t wait_us) {
+  return guarded([&] {
+    if (!s) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "null handle");
+    if (wait_us > 100000) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "wait_us must be at most 100000");
+    std::lock_guard<std::mutex> g(s->mu);
+    std::unique_lock<std::shared_mutex> plan(s->plan_mu);
+    if (!s->tensor_fd()) throw ApiError(VIA_ERR_INVALID_ARGUMENT, "this server's scan has no bounded waits (schoolbook ring)");
+    VIA_CUDA(cudaStreamSynchronize(s->stream));
+    s->fd.fault_wait_ns = wait_us * 1000u;
+    if (wait_us == 0) {  // back to normal: forget the error word of the faulted scans
+      VIA_CUDA(cudaMemsetAsync(s->fd_err.p, 0, 8, s->stream));
+      VIA_CUDA(cudaStreamSynchronize(s->stream));
+    }
+    ++s->plan_gen;  // answer graphs captured with the other setting are re-captured
   });
 }
 

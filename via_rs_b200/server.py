@@ -229,6 +229,11 @@ class Server:
             t = ctypes.byref(_lib.ScanTile(tile.get("n_max", 0), tile.get("stages", 0), tile.get("order", 0), 0))
         check(_lib.lib().via_server_set_scan_tile(self._h, batch, t))
 
+    def set_scan_fault(self, wait_us: int) -> None:
+        """Test hook (via_server_set_scan_fault): scans make a bounded wait run out
+        after wait_us microseconds and report VIA_ERR_TIMEOUT; 0 turns it off."""
+        check(_lib.lib().via_server_set_scan_fault(self._h, wait_us))
+
     def close(self) -> None:
         if self._h:
             _lib.lib().via_server_destroy(self._h)
