@@ -6,7 +6,8 @@ Workload (one step = one answer of one query): the paper VIA-C preset
 4-bit records laid out I=2^8 x J=2^12 (the reference's docs/params.html Table 4
 dimensions for 1 GiB). The prepared database is 10 GiB in HBM (five byte planes
 per eval-form residue, the operand layout of the tensor-core scan), far larger
-than L2, so every step streams it from DRAM.
+than L2, so every step streams it from DRAM. Every step answers a distinct
+query for a seeded index.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
 
@@ -15,6 +16,11 @@ already resident on the device; `e2e` is the same through the host-buffer C ABI
 call via_server_answer (query upload and answer download inside the timed
 region). With N > 1 (torchrun) every rank answers on its own full replica
 ("replicas only": the answer path does not shard), timed as the max over ranks.
+
+Further legs (1 GPU): 64-query shared-scan batches and a Poisson-served stream
+at 1 GiB; VIA-B (T = 8); kernel micro-benchmarks; the scan's roofline; then the
+64-query batched workload at 4 GiB and the served VIA-C / VIA-B mix at 8 GiB;
+last, the CPU oracle on one full-size answer (`cpu_baseline`).
 """
 import argparse
 import ctypes
@@ -62,8 +68,11 @@ def parse():
     ap.add_argument("--served", type=int, default=384,
                     help="requests of the served leg (Poisson arrivals, continuous batching; 0 = skip)")
     ap.add_argument("--via-b", type=int, default=1, help="run the VIA-B leg (T = 8, records of degree 64)")
-    ap.add_argument("--mixed", type=int, default=24, help="requests in the mixed VIA-C / VIA-B served leg (0 = skip)")
+    ap.add_argument("--mixed", type=int, default=32,
+                    help="requests in the mixed VIA-C / VIA-B served leg at 8 GiB (0 = skip)")
     ap.add_argument("--mixed-rate", type=float, default=2.0, help="arrival rate (requests/s) of the mixed leg")
+    ap.add_argument("--big", type=int, default=1,
+                    help="run the 4 GiB batched and 8 GiB mixed legs after the 1 GiB legs (0 = skip)")
     ap.add_argument("--no-autotune", action="store_true", help="keep the default scan tiles (skip the autotuner)")
     ap.add_argument("--microbench", type=int, default=1, help="run the kernel micro-benchmark leg (NTT, external "
                     "product, key switch at n = 2048)")
@@ -150,42 +159,51 @@ class ClockSampler:
 
 
 # ---------------------------------------------------------------------------
-# CPU baseline: the oracle (a restatement of the reference's Rust server) on a
-# bounded sample, extrapolated to the full workload per pipeline stage.
+# CPU baseline: the oracle (a restatement of the reference's Rust server, with
+# its threading: FirstDim over all host threads, the rest serial) answering
+# full-size queries of the same workload. Setup (Server::setup) is not timed.
 # ---------------------------------------------------------------------------
-def cpu_answer_sample(prm, sample_cols=32, seed=7):
+def cpu_server(prm, seed):
     from oracle import pyoracle
 
-    sprm = prm.with_dims(prm.num_rows, sample_cols)
-    records, keys, _ = make_inputs(sprm, seed)
-    rec = np.empty(records.size * 2, dtype=np.uint64)
-    rec[0::2] = records & 15
-    rec[1::2] = records >> 4
+    records, keys, _ = make_inputs(prm, seed)
     threads = os.cpu_count() or 1
-    srv = pyoracle.Server(sprm, keys.cascade_key, keys.conv_key, keys.rsk, rec, threads)
-    q = np.random.default_rng(seed).integers(0, min(prm.q1), size=sprm.n_lwe * sprm.lwe_len, dtype=np.uint64)
-    t0 = time.perf_counter()
-    srv.answer(q)
-    wall = time.perf_counter() - t0
-    st = srv.stage_times()  # decomp, dmux, modswitch, firstdim, cmux, crot, respcomp
-    scale_cols = prm.num_cols / sample_cols
-    t = (st[0] * prm.n_lwe / sprm.n_lwe + st[1] + st[2] + st[3] * scale_cols
-         + st[4] * (prm.num_cols - 1) / (sample_cols - 1) + st[5] + st[6])
-    sample = (f"oracle answer at I={prm.num_rows}, J={sample_cols} ({wall:.2f} s on {threads} threads), "
-              f"stages extrapolated to J={prm.num_cols} and {prm.n_lwe} query LWEs")
-    return t, threads, sample
+    srv = pyoracle.Server(prm, keys.cascade_key, keys.conv_key, keys.rsk, records, threads)
+    del records
+    return srv, threads
+
+
+def cpu_answer_times(srv, prm, count, seed):
+    """Wall seconds of `count` full answers, each of a fresh seeded query."""
+    rng = np.random.default_rng(seed)
+    qmin = min(prm.q1)
+    times = []
+    for _ in range(count):
+        q = rng.integers(0, qmin, size=prm.n_lwe * prm.lwe_len, dtype=np.uint64)
+        t0 = time.perf_counter()
+        srv.answer(q)
+        times.append(time.perf_counter() - t0)
+    return times
+
+
+def cpu_sample_text(prm, threads, n, seconds):
+    return (f"{n} full oracle answer(s) of the workload itself (I={prm.num_rows}, J={prm.num_cols}, "
+            f"{prm.n_lwe} query LWEs, every stage run, no extrapolation): {seconds:.2f} s on {threads} threads; "
+            "setup not timed")
 
 
 def reference_arm(args, prm):
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return
-    times = []
-    threads, sample = 0, ""
-    for i in range(args.warmup + args.steps):
-        t, threads, sample = cpu_answer_sample(prm, seed=7 + i)
-        if i >= args.warmup:
-            times.append(t)
+    try:
+        srv, threads = cpu_server(prm, seed=7)
+    except (MemoryError, RuntimeError) as e:
+        print(json.dumps({"impl": "reference", "unavailable": f"the oracle could not prepare the database: {e}"}),
+              flush=True)
+        return
+    cpu_answer_times(srv, prm, args.warmup, seed=70)
+    times = cpu_answer_times(srv, prm, args.steps, seed=71)
     t_step = sum(times) / len(times)
     value = 1.0 / t_step
     line = {
@@ -194,7 +212,8 @@ def reference_arm(args, prm):
         "scaling": "weak", "vs_baseline": None, "dtype": "u64", "data": "synthetic",
         "config": config_dict(prm),
         "cpu_baseline": {"value": value, "unit": "answers/s", "cores": threads, "kind": "port",
-                         "sample": sample + "; Rust toolchain unavailable, so the C++ oracle restatement is timed"},
+                         "sample": cpu_sample_text(prm, threads, len(times), sum(times))
+                         + "; Rust toolchain unavailable, so the C++ oracle restatement is timed"},
         "e2e": {"value": value, "unit": "answers/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -225,9 +244,41 @@ def max_over_ranks(seconds, dist, device):
     return float(t.item())
 
 
-def served_leg(args, prm, server, query, rate):
-    """Seeded Poisson arrivals at `rate` requests/s into a 2-lane service; returns
-    throughput and the service's p50/p99 submit-to-answer latency."""
+def load_client(prm, seed):
+    """The device client (via_client_*) with seeded ternary secrets: the load
+    generator for distinct, well-formed queries at seeded indices. The server's
+    public keys are seeded residues, not this client's, so the answers do not
+    decrypt; the answer's cost does not depend on key or query values."""
+    from via_rs_b200.client import Client
+
+    rng = np.random.default_rng(seed)
+    t1 = rng.integers(-1, 2, size=prm.nl * prm.n1)
+    sk1 = np.concatenate([np.where(t1[l * prm.n1:(l + 1) * prm.n1] < 0, q + t1[l * prm.n1:(l + 1) * prm.n1],
+                                   t1[l * prm.n1:(l + 1) * prm.n1]).astype(np.uint64)
+                          for l, q in enumerate(prm.q1)])
+    t2 = rng.integers(-1, 2, size=prm.n2)
+    sk2 = np.where(t2 < 0, prm.q3 + t2, t2).astype(np.uint64)
+    return Client(prm, sk1, sk2)
+
+
+def distinct_queries(prm, n, seed, client=None):
+    """n queries for seeded uniform indices, each from its own PRG seed."""
+    own = client is None
+    c = load_client(prm, seed) if own else client
+    idx = np.random.default_rng(seed + 1).integers(prm.capacity, size=n)
+    parts = []
+    for k in range(0, n, 64):
+        chunk = idx[k:k + 64]
+        parts.append(c.queries(chunk, [b"q-%08d-%08d" % (seed, k + j) for j in range(len(chunk))]))
+    if own:
+        c.close()
+    return np.concatenate(parts)
+
+
+def served_leg(args, prm, server, queries, rate):
+    """Seeded Poisson arrivals at `rate` requests/s into a 2-lane service, each
+    request a distinct query; returns throughput and the service's p50/p99
+    submit-to-answer latency."""
     from via_rs_b200.service import Service
 
     rng = np.random.default_rng(7)
@@ -236,17 +287,17 @@ def served_leg(args, prm, server, query, rate):
     # batch size captured up front.
     svc = Service(server, lanes=2, max_batch=64, warm=True, autotune=not args.no_autotune)
     try:
-        for t in [svc.submit(query) for _ in range(4)]:
+        for t in [svc.submit(queries[k]) for k in range(4)]:
             svc.wait(t)
         svc.reset_stats()
         tickets = []
         t0 = time.perf_counter()
         due = t0
-        for g in gaps:
+        for k, g in enumerate(gaps):
             due += g
             while time.perf_counter() < due:
                 time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
-            tickets.append(svc.submit(query))
+            tickets.append(svc.submit(queries[k % len(queries)]))
         for t in tickets:
             svc.wait(t)
         wall = time.perf_counter() - t0
@@ -254,11 +305,199 @@ def served_leg(args, prm, server, query, rate):
         tuning = svc.tuning()
     finally:
         svc.close()
-    return {"requests": args.served, "offered_rate_hz": rate, "answers_s": st["answers_per_s"],
-            "wall_answers_s": args.served / wall, "p50_ms": st["p50_ms"], "p99_ms": st["p99_ms"],
-            "mean_batch": st["mean_batch"], "batches": st["batches"], "lanes": st["lanes"],
+    return {"requests": args.served, "distinct_queries": min(args.served, len(queries)), "offered_rate_hz": rate,
+            "answers_s": st["answers_per_s"], "wall_answers_s": args.served / wall, "p50_ms": st["p50_ms"],
+            "p99_ms": st["p99_ms"], "mean_batch": st["mean_batch"], "batches": st["batches"], "lanes": st["lanes"],
             "max_in_flight": st["max_in_flight"], "arrivals": "seeded Poisson (numpy PCG64 seed 7)",
             "scan_tiles": [{"batch": e["batch"], **e["tile"]} for e in tuning]}
+
+
+def timed_answers(L, server, prm, queries, steps, warmup, stream):
+    """Device-resident answers: one query per step (queries cycled), CUDA events
+    on `stream`. Returns (answers/s, per-step ms)."""
+    import torch
+
+    from via_rs_b200.server import check
+
+    d_q = torch.from_numpy(np.ascontiguousarray(queries).view(np.int64)).cuda()
+    d_m = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
+    d_b = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
+    qlen = prm.n_lwe * prm.lwe_len
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def one(k):
+        check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr() + (k % len(queries)) * qlen * 8),
+                                      prm.n_lwe, ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()),
+                                      sptr))
+
+    for k in range(warmup):
+        one(k)
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for k in range(steps):
+        one(k)
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    return steps / (evs[0].elapsed_time(evs[-1]) / 1e3), ms
+
+
+def timed_batches(L, server, prm, queries, steps, warmup, stream):
+    """Device-resident shared-scan batches of len(queries) distinct queries per
+    step (via_server_answer_many_dev). Returns (answers/s, per-batch ms)."""
+    import torch
+
+    from via_rs_b200.server import check
+
+    B = len(queries)
+    check(L.via_server_reserve(server._h, B))
+    d_qb = torch.from_numpy(np.ascontiguousarray(queries).view(np.int64)).cuda()
+    d_mb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
+    d_bb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
+    sptr = ctypes.c_void_p(stream.cuda_stream)
+
+    def one():
+        check(L.via_server_answer_many_dev(server._h, ctypes.c_void_p(d_qb.data_ptr()), B, prm.n_lwe,
+                                           ctypes.c_void_p(d_mb.data_ptr()), ctypes.c_void_p(d_bb.data_ptr()), sptr))
+
+    for _ in range(warmup):
+        one()
+    torch.cuda.synchronize()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(steps + 1)]
+    evs[0].record(stream)
+    for k in range(steps):
+        one()
+        evs[k + 1].record(stream)
+    torch.cuda.synchronize()
+    ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(steps)]
+    return steps * B / (evs[0].elapsed_time(evs[-1]) / 1e3), ms
+
+
+def batched_4gib_leg(args, seed):
+    """The batched workload at 4 GiB (I = 2^9, J = 2^13): plain answers, then
+    shared-scan batches of `--batch` distinct seeded-index queries, tuned scan."""
+    import torch
+
+    from via_rs_b200 import _lib
+    from via_rs_b200.params import paper_preset
+    from via_rs_b200.server import VIA_RECORDS_NIBBLE, Server
+
+    prm = paper_preset(512, 8192)
+    L = _lib.lib()
+    records, keys, _ = make_inputs(prm, seed)
+    server = Server.setup(prm, keys, records, VIA_RECORDS_NIBBLE)
+    del records
+    B = args.batch
+    queries = distinct_queries(prm, B, seed=seed + 1)
+    tuning = [] if args.no_autotune else server.autotune([1, B])
+    stream = torch.cuda.Stream()
+    plain, plain_ms = timed_answers(L, server, prm, queries, steps=8, warmup=3, stream=stream)
+    batched, b_ms = timed_batches(L, server, prm, queries, steps=3, warmup=1, stream=stream)
+    db = prepared_db_bytes(prm)
+    server.close()
+    del server
+    torch.cuda.empty_cache()
+    return {"db_raw_bytes": prm.capacity * prm.n_rec // 2, "rows": prm.num_rows, "cols": prm.num_cols,
+            "db_prepared_bytes": db, "batch": B, "distinct_queries": B,
+            "plain_answers_s": plain, "plain_p50_ms": float(np.percentile(plain_ms, 50)),
+            "plain_db_gbs": plain * db / 1e9,
+            "answers_s": batched, "ms_per_batch": float(np.mean(b_ms)), "p50_ms": float(np.percentile(b_ms, 50)),
+            "p99_ms": float(np.percentile(b_ms, 99)), "db_gbs": batched * db / 1e9 / B,
+            "vs_plain": batched / plain, "autotune": tuning}
+
+
+def mixed_8gib_leg(args, seed):
+    """The served mixed load at 8 GiB (I = 2^10, J = 2^13): a seeded Poisson
+    stream of VIA-C queries and VIA-B requests of 1..256 indices (log-uniform),
+    each VIA-B request padded to the smallest power-of-two batch T >= m and
+    served from views of the one prepared database (a continuous-batching
+    service per view, admitted by an HBM budget). Every request carries
+    distinct queries; one request per route is re-answered alone and compared."""
+    import torch
+
+    from via_rs_b200 import _lib
+    from via_rs_b200.mixed import MixedService, poisson_mix, via_b_route
+    from via_rs_b200.params import paper_preset
+    from via_rs_b200.server import VIA_RECORDS_NIBBLE, Server
+
+    prm = paper_preset(1024, 8192)
+    L = _lib.lib()
+    records, keys, _ = make_inputs(prm, seed)
+    server = Server.setup(prm, keys, records, VIA_RECORDS_NIBBLE)
+    del records
+    stream = torch.cuda.Stream()
+    plain_q = distinct_queries(prm, 4, seed=seed + 1)
+    if not args.no_autotune:
+        server.autotune([1])
+    plain, _ = timed_answers(L, server, prm, plain_q, steps=4, warmup=2, stream=stream)
+    free, _ = torch.cuda.mem_get_info()
+    budget = int(free * 0.6)
+    t_build = time.perf_counter()
+    mix = MixedService(server, lanes=2, hbm_budget=budget, autotune=not args.no_autotune)
+    t_build = time.perf_counter() - t_build
+    clients = {}
+
+    def queries(route, n_req):
+        pv = mix.params(route)
+        if route not in clients:
+            clients[route] = load_client(pv, seed + 100 + (0 if route == "c" else route))
+        return distinct_queries(pv, 1 if route == "c" else route, seed=seed + 1000 + n_req, client=clients[route])
+
+    plan = []
+    for k, (gap, kind, m) in enumerate(poisson_mix(args.mixed, args.mixed_rate, seed=22)):
+        route = "c" if kind == "c" else via_b_route(m)
+        plan.append((gap, route, m, queries(route, k)))
+    for c in clients.values():
+        c.close()
+    routes = sorted({p[1] for p in plan}, key=str)
+    try:
+        for route in routes:  # one warm request per route in the stream
+            mix.wait(mix.submit(route, next(p[3] for p in plan if p[1] == route)))
+        mix.reset_stats()
+        handles = []
+        t0 = time.perf_counter()
+        due = t0
+        for gap, route, m, q in plan:
+            due += gap
+            while time.perf_counter() < due:
+                time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
+            handles.append(mix.submit(route, q))
+        answers = [mix.wait(h) for h in handles]
+        wall = time.perf_counter() - t0
+        lat = mix.latencies()
+        mix.close_services()  # frees the lanes before the views answer alone
+        exact = True
+        for route in routes:
+            k = next(i for i, p in enumerate(plan) if p[1] == route)
+            srv = mix.servers[route]
+            alone = srv.answer(plan[k][3]) if route == "c" else srv.answer_batch(plan[k][3].reshape(route, -1))
+            exact = exact and np.array_equal(alone[0], answers[k][0]) and np.array_equal(alone[1], answers[k][1])
+    finally:
+        mix.close()
+        server.close()
+        del server
+        torch.cuda.empty_cache()
+    n_c = sum(1 for p in plan if p[1] == "c")
+    b = [p for p in plan if p[1] != "c"]
+    records_n = n_c + sum(p[2] for p in b)
+    slots = sum(p[1] for p in b)
+    all_lat = np.concatenate([v for v in lat.values() if len(v)])
+
+    def pct(v, q):
+        return float(np.percentile(v, q)) if len(v) else None
+
+    return {"db_raw_bytes": prm.capacity * prm.n_rec // 2, "rows": prm.num_rows, "cols": prm.num_cols,
+            "db_prepared_bytes": prepared_db_bytes(prm), "plain_answers_s": plain,
+            "requests": len(plan), "via_c": n_c, "via_b": len(b),
+            "via_b_by_t": {str(t): sum(1 for p in b if p[1] == t) for t in routes if t != "c"},
+            "offered_rate_hz": args.mixed_rate, "requests_s": len(plan) / wall, "answers_s": len(plan) / wall,
+            "records_s": records_n / wall, "padding_frac": (slots - sum(p[2] for p in b)) / max(1, slots),
+            "p50_ms": pct(all_lat, 50), "p99_ms": pct(all_lat, 99),
+            "p50_ms_by_route": {str(k): pct(v, 50) for k, v in lat.items() if len(v)},
+            "p99_ms_by_route": {str(k): pct(v, 99) for k, v in lat.items() if len(v)},
+            "hbm_budget_bytes": budget, "services_build_s": t_build, "sampled_bit_exact": bool(exact),
+            "arrivals": "seeded Poisson (numpy PCG64 seed 22), half VIA-C, VIA-B sizes log-uniform in 1..256"}
 
 
 def microbench_leg(args, prm, peak):
@@ -330,16 +569,8 @@ def microbench_leg(args, prm, peak):
 def client_microbench(prm):
     """Device client at the bench's preset and grid: 64 queries generated per call
     (one seeded PRG stream each) and 256 answers recovered per call."""
-    from via_rs_b200.client import Client
-
     rng = np.random.default_rng(13)
-    ternary = rng.integers(-1, 2, size=prm.nl * prm.n1)
-    sk1 = np.concatenate([np.where(ternary[l * prm.n1:(l + 1) * prm.n1] < 0, q + ternary[l * prm.n1:(l + 1) * prm.n1],
-                                   ternary[l * prm.n1:(l + 1) * prm.n1]).astype(np.uint64)
-                          for l, q in enumerate(prm.q1)])
-    s2 = rng.integers(-1, 2, size=prm.n2)
-    sk2 = np.where(s2 < 0, prm.q3 + s2, s2).astype(np.uint64)
-    c = Client(prm, sk1, sk2)
+    c = load_client(prm, 13)
     n = 64
     idx = rng.integers(prm.capacity, size=n)
     seeds = [b"bench-%04d" % k for k in range(n)]
@@ -359,78 +590,6 @@ def client_microbench(prm):
             "timing": "host wall clock around the synchronous call (host buffers, copies included)"}
 
 
-def mixed_leg(args, prm, server, rate):
-    """A seeded Poisson stream of VIA-C queries and VIA-B requests of 1..256
-    indices (log-uniform), padded to T = 8 (records of degree 64) or T = 256
-    (degree 2), served from the one prepared database through three views with a
-    continuous-batching service each. Returns throughput, padding and p50/p99;
-    one request of each kind is re-answered alone and compared."""
-    import torch
-
-    from via_rs_b200.mixed import MixedService, poisson_mix, via_b_route
-
-    free, _ = torch.cuda.mem_get_info()
-    budget = int(free * 0.6)
-    mix = MixedService(server, lanes=2, hbm_budget=budget, shares={"c": 0.35, 8: 0.15, 256: 0.5},
-                       autotune=not args.no_autotune)
-    rng = np.random.default_rng(21)
-    qmin = min(prm.q1)
-
-    def queries(route):
-        pv = mix.params(route)
-        count = 1 if route == "c" else route
-        return rng.integers(0, qmin, size=count * pv.n_lwe * pv.lwe_len, dtype=np.uint64)
-
-    plan = []
-    for gap, kind, m in poisson_mix(args.mixed, rate, seed=22):
-        route = "c" if kind == "c" else via_b_route(m)
-        plan.append((gap, route, m, queries(route)))
-    try:
-        for route in ("c", 8, 256):  # one warm request per route
-            mix.wait(mix.submit(route, queries(route)))
-        mix.reset_stats()
-        handles = []
-        t0 = time.perf_counter()
-        due = t0
-        for gap, route, m, q in plan:
-            due += gap
-            while time.perf_counter() < due:
-                time.sleep(min(0.0005, max(0.0, due - time.perf_counter())))
-            handles.append(mix.submit(route, q))
-        answers = [mix.wait(h) for h in handles]
-        wall = time.perf_counter() - t0
-        lat = mix.latencies()
-        mix.close_services()  # frees the lanes before the views answer alone
-        exact = True
-        for route in ("c", 8, 256):
-            k = next((i for i, p in enumerate(plan) if p[1] == route), None)
-            if k is None:
-                continue
-            srv = mix.servers[route]
-            alone = srv.answer(plan[k][3]) if route == "c" else srv.answer_batch(plan[k][3].reshape(route, -1))
-            exact = exact and np.array_equal(alone[0], answers[k][0]) and np.array_equal(alone[1], answers[k][1])
-    finally:
-        mix.close()
-    n_c = sum(1 for p in plan if p[1] == "c")
-    b = [p for p in plan if p[1] != "c"]
-    records = n_c + sum(p[2] for p in b)
-    slots = sum(p[1] for p in b)
-    all_lat = np.concatenate([v for v in lat.values() if len(v)])
-
-    def pct(v, q):
-        return float(np.percentile(v, q)) if len(v) else None
-
-    return {"requests": len(plan), "via_c": n_c, "via_b_t8": sum(1 for p in b if p[1] == 8),
-            "via_b_t256": sum(1 for p in b if p[1] == 256), "offered_rate_hz": rate,
-            "requests_s": len(plan) / wall, "records_s": records / wall,
-            "answers_s": len(plan) / wall, "padding_frac": (slots - sum(p[2] for p in b)) / max(1, slots),
-            "p50_ms": pct(all_lat, 50), "p99_ms": pct(all_lat, 99),
-            "p50_ms_by_route": {str(k): pct(v, 50) for k, v in lat.items()},
-            "p99_ms_by_route": {str(k): pct(v, 99) for k, v in lat.items()},
-            "hbm_budget_bytes": budget, "sampled_bit_exact": bool(exact),
-            "arrivals": "seeded Poisson (numpy PCG64 seed 22), half VIA-C, VIA-B sizes log-uniform in 1..256"}
-
-
 def via_b_leg(args, prm, rank):
     """answer_batch with T = n2 / n3 = 8 queries per answer over the same number
     of database cells (records of degree 64: 8x the records of the VIA-C leg)."""
@@ -442,11 +601,11 @@ def via_b_leg(args, prm, rank):
 
     pb = paper_preset(prm.num_rows, prm.num_cols, n_rec=64)
     T = pb.n2 // pb.n_rec
-    records, keys, query = make_inputs(pb, seed=100 + rank)
+    records, keys, _ = make_inputs(pb, seed=100 + rank)
     srv = Server.setup(pb, keys, records, VIA_RECORDS_NIBBLE)
     del records
     L = _lib.lib()
-    qs = torch.from_numpy(np.tile(query, T).view(np.int64)).cuda()
+    qs = torch.from_numpy(distinct_queries(pb, T, seed=200 + rank).view(np.int64)).cuda()
     dm = torch.empty(pb.n2, dtype=torch.int64, device="cuda")
     db = torch.empty(pb.n2, dtype=torch.int64, device="cuda")
     stream = torch.cuda.Stream()
@@ -496,13 +655,18 @@ def gpu_arm(args, prm):
     del records
     stream = torch.cuda.Stream()
     sptr = ctypes.c_void_p(stream.cuda_stream)
-    d_q = torch.from_numpy(query.view(np.int64)).cuda()
+    # Distinct well-formed queries at seeded indices (the device client).
+    n_distinct = max(args.steps, args.batch, min(args.served, 384), 1)
+    queries = distinct_queries(prm, n_distinct, seed=1000 + rank)
+    qlen = prm.n_lwe * prm.lwe_len
+    d_q = torch.from_numpy(queries[:args.steps].view(np.int64)).cuda()
     d_m = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
     d_b = torch.empty(prm.n2, dtype=torch.int64, device="cuda")
 
-    def answer_dev():
-        check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr()), prm.n_lwe,
-                                      ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()), sptr))
+    def answer_dev(k):
+        check(L.via_server_answer_dev(server._h, ctypes.c_void_p(d_q.data_ptr() + (k % args.steps) * qlen * 8),
+                                      prm.n_lwe, ctypes.c_void_p(d_m.data_ptr()), ctypes.c_void_p(d_b.data_ptr()),
+                                      sptr))
 
     # Scan autotuner: the fastest tile for one query and for the batched leg.
     tuning = []
@@ -511,18 +675,17 @@ def gpu_arm(args, prm):
 
     if args.profile_batch:
         B = max(1, args.batch)
-        qb = np.tile(query, B)
-        mb, bb = server.answer_many(qb.reshape(B, -1))
+        mb, bb = server.answer_many(queries[:B])
         torch.cuda.synchronize()
         print(json.dumps({"profile_batch": B, "answers": int(mb.shape[0])}), flush=True)
         server.close()
         return
 
-    for _ in range(args.warmup):
-        answer_dev()
+    for k in range(args.warmup):
+        answer_dev(k)
     torch.cuda.synchronize()
 
-    # ---- timed region: K device-resident answers.
+    # ---- timed region: K device-resident answers, one distinct query each.
     clocks = ClockSampler(local)
     clocks.start()
     time.sleep(0.3)
@@ -534,7 +697,7 @@ def gpu_arm(args, prm):
     with torch.cuda.stream(stream):
         evs[0].record(stream)
         for k in range(args.steps):
-            answer_dev()
+            answer_dev(k)
             evs[k + 1].record(stream)
     torch.cuda.synchronize()
     launches = L.via_kernel_launches() - l0
@@ -549,63 +712,37 @@ def gpu_arm(args, prm):
     db_bytes = prepared_db_bytes(prm)
 
     # ---- e2e: the reference-facing host-buffer call, copies inside the region.
-    for _ in range(2):
-        server.answer(query)
+    for k in range(2):
+        server.answer(queries[k])
     if dist:
         dist.barrier()
     torch.cuda.synchronize()
     t0 = time.perf_counter()
-    for _ in range(args.steps):
-        server.answer(query)
+    for k in range(args.steps):
+        server.answer(queries[k])
     e2e_el = time.perf_counter() - t0
     e2e_el = max_over_ranks(e2e_el, dist, "cuda")
     e2e_value = n_answers / e2e_el
 
-    # ---- batched: B independent queries per step share one database pass.
+    # ---- batched: B distinct queries per step share one database pass.
     batched = None
     if args.batch > 1:
         B = args.batch
-        check(L.via_server_reserve(server._h, B))
-        qb = np.tile(query, B)
-        d_qb = torch.from_numpy(qb.view(np.int64)).cuda()
-        d_mb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
-        d_bb = torch.empty(B * prm.n2, dtype=torch.int64, device="cuda")
-
-        def answer_many():
-            check(L.via_server_answer_many_dev(server._h, ctypes.c_void_p(d_qb.data_ptr()), B, prm.n_lwe,
-                                               ctypes.c_void_p(d_mb.data_ptr()), ctypes.c_void_p(d_bb.data_ptr()),
-                                               sptr))
-
-        for _ in range(2):
-            answer_many()
         kb = max(2, args.steps // 4)
-        bev = [torch.cuda.Event(enable_timing=True) for _ in range(kb + 1)]
         if dist:
             dist.barrier()
-        torch.cuda.synchronize()
-        bev[0].record(stream)
-        for k in range(kb):
-            answer_many()
-            bev[k + 1].record(stream)
-        torch.cuda.synchronize()
-        b_ms = [bev[k].elapsed_time(bev[k + 1]) for k in range(kb)]
-        b_el = bev[0].elapsed_time(bev[-1]) / 1e3
-        b_el = max_over_ranks(b_el, dist, "cuda")
+        b_value, b_ms = timed_batches(L, server, prm, queries[:B], steps=kb, warmup=2, stream=stream)
+        b_el = max_over_ranks(kb * B / b_value, dist, "cuda")
         b_value = kb * B * world / b_el
-        batched = {"answers_s": b_value, "batch": B, "steps": kb, "ms_per_batch": b_el / kb * 1e3,
-                   "db_gbs": b_value * db_bytes / 1e9 / B, "p50_ms": float(np.percentile(b_ms, 50)),
-                   "p99_ms": float(np.percentile(b_ms, 99)), "vs_plain": b_value / value}
-        del d_qb, d_mb, d_bb
+        batched = {"answers_s": b_value, "batch": B, "distinct_queries": B, "steps": kb,
+                   "ms_per_batch": b_el / kb * 1e3, "db_gbs": b_value * db_bytes / 1e9 / B,
+                   "p50_ms": float(np.percentile(b_ms, 50)), "p99_ms": float(np.percentile(b_ms, 99)),
+                   "vs_plain": b_value / value}
 
-    # ---- served: Poisson arrivals through the continuous-batching service.
+    # ---- served: Poisson arrivals of distinct queries through the service.
     served = None
     if args.served > 0:
-        served = served_leg(args, prm, server, query, rate=0.85 * (batched["answers_s"] if batched else value))
-
-    # ---- mixed VIA-C / VIA-B stream over views of the same database.
-    mixed = None
-    if args.mixed > 0 and world == 1:
-        mixed = mixed_leg(args, prm, server, args.mixed_rate)
+        served = served_leg(args, prm, server, queries, rate=0.85 * (batched["answers_s"] if batched else value))
 
     # ---- VIA-B: T = 8 records of degree 64 per answer on a second (1 GiB) server.
     via_b = None
@@ -635,21 +772,30 @@ def gpu_arm(args, prm):
     scan_bytes = db_bytes + sel.numel() * 8 + out.numel() * 8
     peak, peak_kind = load_peaks()
     achieved = scan_bytes / scan_s / 1e9
+    server.close()
+    del server, d_q, sel, out
+    torch.cuda.empty_cache()
+
+    # ---- the configs' larger databases (1 GPU): 4 GiB batched, 8 GiB served mix.
+    big4 = batched_4gib_leg(args, seed=40 + rank) if args.big and world == 1 and args.batch > 1 else None
+    mixed8 = mixed_8gib_leg(args, seed=80 + rank) if args.big and world == 1 and args.mixed > 0 else None
 
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "answers/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": elapsed / args.steps * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u64",
-            "data": "synthetic: seeded uniform 4-bit records (numpy PCG64), uniform key/query residues",
+            "data": "synthetic: seeded uniform 4-bit records (numpy PCG64), seeded key residues, distinct device-client "
+                    "queries at seeded indices",
             "config": config_dict(prm),
             "plain": {"answers_s": value, "db_gbs": value * db_bytes / 1e9, "db_raw_gbs": value * (1 << 30) / 1e9,
                       "p50_ms": float(np.percentile(step_ms, 50)), "p99_ms": float(np.percentile(step_ms, 99))},
             "batched": batched,
             "served": served,
             "via_b": via_b,
+            "batched_4gib": big4,
+            "mixed_8gib": mixed8,
             "microbench": micro,
-            "mixed": mixed,
             "roofline": {"bound": "hbm", "kernel": "k_fd_split + k_fd_tc (tcgen05 FirstDim scan)", "achieved": achieved,
                          "peak": peak, "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
                          "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols
@@ -662,11 +808,12 @@ def gpu_arm(args, prm):
             "clocks": clk,
         }
         if world == 1 and not args.no_cpu_baseline:
-            t, threads, sample = cpu_answer_sample(prm)
-            line["cpu_baseline"] = {"value": 1.0 / t, "unit": "answers/s", "cores": threads, "kind": "port",
-                                    "sample": sample}
+            srv, threads = cpu_server(prm, seed=7)
+            t = cpu_answer_times(srv, prm, 1, seed=71)
+            del srv
+            line["cpu_baseline"] = {"value": 1.0 / t[0], "unit": "answers/s", "cores": threads, "kind": "port",
+                                    "sample": cpu_sample_text(prm, threads, 1, t[0])}
         print(json.dumps(line), flush=True)
-    server.close()
     if dist:
         dist.destroy_process_group()
 
