@@ -225,7 +225,7 @@ via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, 
  * threaded CPU loop.
  */
 typedef struct via_scan_tile {
-  uint32_t n_max;    /* selection columns per tile for batches: 16, 32 or 48; 0 = default (48) */
+  uint32_t n_max;    /* selection columns per tile for batches: 16, 24, 32 or 48; 0 = default (48) */
   uint32_t stages;   /* shared-memory ring depth, 2..6; 0 = default (3; 4 for one query) */
   uint32_t order;    /* 0: slot-major units, 1: tile-major units (batches only) */
   uint32_t reserved;

@@ -340,8 +340,9 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
         const int j = jt * FD_MT + row;
         const bool jok = j < P.J;
         if (P.grouped) {
-          const int c_lo = half * (P.N / 2), c_hi = c_lo + P.N / 2;
-          for (int c0 = c_lo; c0 < c_hi; c0 += 8) {
+          // 8-column chunks of the tile, alternating between the two halves
+          // (N is a multiple of 8).
+          for (int c0 = half * 8; c0 < P.N; c0 += 16) {
             u32 v[9][8];
 #pragma unroll
             for (int g = 0; g < 9; ++g) tmem_ld8(tb + (u32)(g * P.N + c0), v[g]);
@@ -406,18 +407,29 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
 
 // Split selection: [t][ct][kc][Np x 64 bytes, core-matrix order], row l*N + c
 // holding byte l of column c (query b = cg/2, mask or body = cg%2) of the
-// c-tile. One thread per (t, ct, c, 16 consecutive rows i).
+// c-tile. One thread per (t, ct, c, 16 consecutive rows i). Grouped tiles whose
+// 5N is not a multiple of 16 pad the operand to Np rows: rows 5N .. Np-1 are
+// written as zeros (they reach accumulator columns that are read), one thread
+// per padding row as the virtual columns c = N .. N + Np - 5N - 1.
 __global__ void k_fd_split(const u64* __restrict__ sel, int nq, int I, int n, int n_k16, int n_kc, int n_ct, int N,
-                           int Np, uint8_t* __restrict__ out) {
-  const long total = (long)n * n_ct * N * n_k16;
+                           int Np, int pad, uint8_t* __restrict__ out) {
+  const int NC = N + pad;  // pad: zero rows of a grouped tile
+  const long total = (long)n * n_ct * NC * n_k16;
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= total) return;
   const int t = (int)(gid % n);
   long r = gid / n;
   const int k16 = (int)(r % n_k16);
   r /= n_k16;
-  const int c = (int)(r % N);
-  const int ct = (int)(r / N);
+  const int c = (int)(r % NC);
+  const int ct = (int)(r / NC);
+  if (c >= N) {
+    const int kc = k16 / (FD_KC / 16), kk = k16 % (FD_KC / 16);
+    uint8_t* base = out + (((size_t)t * n_ct + ct) * n_kc + kc) * ((size_t)Np * FD_KC);
+    const int rr = FD_LIMBS * N + (c - N);
+    *reinterpret_cast<uint4*>(base + ((size_t)kk * (Np / 8) + rr / 8) * 128 + (rr % 8) * 16) = make_uint4(0, 0, 0, 0);
+    return;
+  }
   const int cg = ct * N + c;
   const bool valid = cg < 2 * nq;
   const int b = cg >> 1, mb = cg & 1;
@@ -489,11 +501,14 @@ Tiling tiling(int nq, const FdTile& tile) {
     const int cap = tile.n_max ? tile.n_max : 48;
     T.grouped = 1;
     T.n_ct = (2 * nq + cap - 1) / cap;
-    T.N = fd_round_up((2 * nq + T.n_ct - 1) / T.n_ct, 16);
-    T.Np = FD_LIMBS * T.N;
+    // n_max = 24 tiles round N to 8 and pad the MMA operand to a multiple of 16
+    // rows, so that two accumulator sets (up to 224 columns each) fit in TMEM.
+    T.N = fd_round_up((2 * nq + T.n_ct - 1) / T.n_ct, cap == 24 ? 8 : 16);
+    T.Np = fd_round_up(FD_LIMBS * T.N, 16);
     T.stages = tile.stages ? tile.stages : 3;
     T.order = tile.order;
-    acc_cols = 9 * T.N;
+    // Limb k's MMA writes columns [k N, k N + Np); the epilogue reads [0, 9 N).
+    acc_cols = std::max(9 * T.N, 4 * T.N + T.Np);
   }
   T.acc_stride = fd_round_up(acc_cols, 32);
   T.nacc = 2 * T.acc_stride <= 512 ? 2 : 1;
@@ -517,7 +532,7 @@ bool fd_supported(int I, int n, u64 q) { return I >= 1 && I <= 4096 && n >= 1 &&
 
 bool fd_tile_valid(const FdPlan& p, int nq, const FdTile& t) {
   if (nq < 1) return false;
-  if (t.n_max != 0 && t.n_max != 16 && t.n_max != 32 && t.n_max != 48) return false;
+  if (t.n_max != 0 && t.n_max != 16 && t.n_max != 24 && t.n_max != 32 && t.n_max != 48) return false;
   if (t.stages != 0 && (t.stages < 2 || t.stages > 6)) return false;
   if (t.order != 0 && t.order != 1) return false;
   if (nq == 1 && (t.n_max != 0 || t.order != 0)) return false;
@@ -562,7 +577,7 @@ std::vector<FdTile> fd_tile_candidates(const FdPlan& p, int nq) {
   if (nq == 1) {
     for (int st = 2; st <= 6; ++st) add(FdTile{0, st, 0});
   } else {
-    for (int nm : {16, 32, 48})
+    for (int nm : {16, 24, 32, 48})
       for (int st = 2; st <= 5; ++st)
         for (int od = 0; od <= 1; ++od) add(FdTile{nm, st, od});
   }
@@ -601,8 +616,9 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
   if (force && !fd_tile_valid(p, nq, tile)) throw CudaError(100, "scan tile not valid for this batch");
   const Tiling T = tiling(nq, tile);
   const int n_k16 = p.I_pad / 16, n_kc = p.I_pad / FD_KC;
-  const long total = (long)p.n * T.n_ct * T.N * n_k16;
-  k_fd_split<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(sel_eval, nq, p.I, p.n, n_k16, n_kc, T.n_ct, T.N, T.Np,
+  const int pad = T.grouped ? T.Np - FD_LIMBS * T.N : 0;
+  const long total = (long)p.n * T.n_ct * (T.N + pad) * n_k16;
+  k_fd_split<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(sel_eval, nq, p.I, p.n, n_k16, n_kc, T.n_ct, T.N, T.Np, pad,
                                                               scratch);
   VIA_LAUNCHED();
   KParams K;

@@ -30,9 +30,12 @@ constexpr int FD_CHUNK = FD_LIMBS * FD_MT * FD_KC;  // 40960 bytes
 
 // One scan tile choice, the autotuner's search space. Every choice computes the
 // same exact sums; they differ in speed only.
-//  n_max  : selection columns per c-tile for batches (16, 32 or 48); the
+//  n_max  : selection columns per c-tile for batches (16, 24, 32 or 48); the
 //           batch's 2*nq columns are spread evenly over ceil(2nq / n_max)
-//           tiles, each padded to a multiple of 16. Ignored for one query.
+//           tiles, each padded to a multiple of 16 (of 8 for n_max = 24, whose
+//           MMA operand is padded with zero rows to a multiple of 16). Tiles of
+//           at most 24 columns hold two accumulator sets in TMEM, so the MMAs of
+//           one column tile overlap the epilogue of the previous one.
 //  stages : depth of the shared-memory ring of (database, selection) chunks.
 //  order  : 0 walks units slot-major (the c-tiles of one slot run on
 //           neighbouring SMs at the same time and share the slot's planes in
