@@ -473,6 +473,8 @@ def mixed_8gib_leg(args, seed):
             srv = mix.servers[route]
             alone = srv.answer(plan[k][3]) if route == "c" else srv.answer_batch(plan[k][3].reshape(route, -1))
             exact = exact and np.array_equal(alone[0], answers[k][0]) and np.array_equal(alone[1], answers[k][1])
+            if route != "c":  # each view's own workspace goes before the next view answers
+                mix.servers.pop(route).close()
     finally:
         mix.close()
         server.close()
@@ -631,6 +633,11 @@ def via_b_leg(args, prm, rank):
             "records_s": T * 1e3 / ms, "db_raw_bytes": pb.capacity * pb.n_rec // 2}
 
 
+def log_leg(name, result):
+    """Each finished leg on stderr (the JSON line on stdout comes at the end)."""
+    print(json.dumps({"leg": name, "result": result}), file=sys.stderr, flush=True)
+
+
 def gpu_arm(args, prm):
     import torch
 
@@ -777,8 +784,13 @@ def gpu_arm(args, prm):
     torch.cuda.empty_cache()
 
     # ---- the configs' larger databases (1 GPU): 4 GiB batched, 8 GiB served mix.
+    log_leg("plain", {"answers_s": value, "e2e": e2e_value, "scan_ms": scan_s * 1e3})
+    log_leg("batched", batched)
+    log_leg("served", served)
     big4 = batched_4gib_leg(args, seed=40 + rank) if args.big and world == 1 and args.batch > 1 else None
+    log_leg("batched_4gib", big4)
     mixed8 = mixed_8gib_leg(args, seed=80 + rank) if args.big and world == 1 and args.mixed > 0 else None
+    log_leg("mixed_8gib", mixed8)
 
     if rank == 0:
         line = {
