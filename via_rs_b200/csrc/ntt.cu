@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "ntt.cuh"
+#include "ntt_fp.cuh"
 
 namespace via {
 
@@ -66,7 +67,7 @@ NttTableHost make_ntt_table(u64 q, int nmax) {
   }
   int logn = __builtin_ctz((unsigned)nmax);
   u64 ipsi = h_pow(psi, q - 2, q);
-  std::vector<u64> host(4 * (size_t)nmax);
+  std::vector<u64> host(6 * (size_t)nmax);
   for (int k = 0; k < nmax; ++k) {
     u64 w = h_pow(psi, (u64)bitrev(k, logn), q);
     u64 wi = h_pow(ipsi, (u64)bitrev(k, logn), q);
@@ -74,6 +75,9 @@ NttTableHost make_ntt_table(u64 q, int nmax) {
     host[nmax + k] = (u64)(((u128)w << 64) / q);
     host[2 * nmax + k] = wi;
     host[3 * nmax + k] = (u64)(((u128)wi << 64) / q);
+    const double wd = (double)w, wid = (double)wi;  // exact: w, wi < q < 2^50
+    std::memcpy(&host[4 * nmax + k], &wd, 8);
+    std::memcpy(&host[5 * nmax + k], &wid, 8);
   }
   VIA_CUDA(cudaMalloc(&h.buf, host.size() * 8));
   VIA_CUDA(cudaMemcpy(h.buf, host.data(), host.size() * 8, cudaMemcpyHostToDevice));
@@ -83,10 +87,15 @@ NttTableHost make_ntt_table(u64 q, int nmax) {
   h.dev.psi_sh = h.buf + nmax;
   h.dev.ipsi = h.buf + 2 * nmax;
   h.dev.ipsi_sh = h.buf + 3 * nmax;
+  h.dev.psi_d = reinterpret_cast<const double*>(h.buf + 4 * nmax);
+  h.dev.ipsi_d = reinterpret_cast<const double*>(h.buf + 5 * nmax);
+  h.dev.qd = (double)q;
+  h.dev.qinv = 1.0 / (double)q;
   for (int l = 0; l <= NTT_MAX_LOGN; ++l) {
     u64 ninv = h_pow((u64)1 << l, q - 2, q);
     h.dev.ninv[l] = ninv;
     h.dev.ninv_sh[l] = (u64)(((u128)ninv << 64) / q);
+    h.dev.ninv_d[l] = (double)ninv;
   }
   h.valid = true;
   return h;
@@ -198,6 +207,58 @@ __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg_i8(const int8_t* __
   u64 e[8];
   ntt_phases<LOGN, false, 0, true, true>(e, tid, T, out + seg * n, sm, seg_local * n, active,
                                          din + (active ? seg / nl : 0) * n);
+}
+
+// k_ntt_reg_i8 in double precision (ntt_fp.cuh): the digits (|d| <= 127) are
+// transformed as exact integer doubles; the outputs, within 0.5625 LOGN q + 127
+// of zero, are offset by OFF q (OFF = ceil(0.5625 LOGN) + 1) to a nonnegative
+// residue below (1.125 LOGN + 3) q <= (1 + 2 LOGN) q, the bound of the integer
+// kernel's lazy outputs, and stored as u64. Primes below 2^44 (values stay far
+// below 2^48).
+template <int LOGN, int P>
+__device__ __forceinline__ void ntt_fp_phases_i8(double (&e)[8], int tid, const NttTable& T, u64* g, double* sm,
+                                                 int sbase, bool active) {
+  using Ph = NttPhaseFp<LOGN, false, P>;
+  using Ix = NttPhase<LOGN, false, P>;
+  constexpr int NPH = (LOGN + 2) / 3;
+  if (P > 0) {
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) e[v] = sm[swz(sbase + Ix::index(v, tid))];
+  }
+  Ph::run(e, tid, T);
+  if constexpr (P == NPH - 1) {
+    constexpr int OFF = (9 * LOGN + 15) / 16 + 1;  // ceil(0.5625 LOGN) + 1
+    const double off = (double)OFF * T.qd;
+    if (active) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) g[Ix::index(v, tid)] = __double2ull_rn(__dadd_rn(e[v], off));
+    }
+  } else {
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) sm[swz(sbase + Ix::index(v, tid))] = e[v];
+    ntt_fp_phases_i8<LOGN, P + 1>(e, tid, T, g, sm, sbase, active);
+  }
+}
+
+template <int LOGN>
+__global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_fp_i8(const int8_t* __restrict__ din, u64* __restrict__ out,
+                                                               int nl, long segments, NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  constexpr int TPS = n / 8;
+  constexpr int SPC = ntt_cta<LOGN>() / TPS;
+  __shared__ double sm[ntt_cta<LOGN>() * 8];
+  const int seg_local = threadIdx.x / TPS;
+  const int tid = threadIdx.x % TPS;
+  const long seg = (long)blockIdx.x * SPC + seg_local;
+  const bool active = seg < segments;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  const int8_t* gin = din + (active ? seg / nl : 0) * n;
+  double e[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) e[v] = active ? (double)gin[NttPhase<LOGN, false, 0>::index(v, tid)] : 0.0;
+  ntt_fp_phases_i8<LOGN, 0>(e, tid, T, out + seg * n, sm, seg_local * n, active);
 }
 
 // n = 2 and 4 on 8-bit digits: one thread per segment.
@@ -331,9 +392,16 @@ void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segmen
   const int cta = std::max(NTT_THREADS, n / 8);
   const long spc = cta / (n / 8);
   const unsigned blocks = (unsigned)((segments + spc - 1) / spc);
+  // Double precision when both primes are below 2^44 (exact products, see ntt_fp.cuh).
+  const bool fp = t0.q < (1ull << 44) && t1.q < (1ull << 44);
   switch (logn) {
-#define VIA_NTT_I8_CASE(LG) \
-  case LG: k_ntt_reg_i8<LG><<<blocks, cta, 0, st>>>(din, out, nl, segments, t0, t1); break;
+#define VIA_NTT_I8_CASE(LG)                                                            \
+  case LG:                                                                             \
+    if (fp)                                                                            \
+      k_ntt_fp_i8<LG><<<blocks, cta, 0, st>>>(din, out, nl, segments, t0, t1);         \
+    else                                                                               \
+      k_ntt_reg_i8<LG><<<blocks, cta, 0, st>>>(din, out, nl, segments, t0, t1);        \
+    break;
     VIA_NTT_I8_CASE(3)
     VIA_NTT_I8_CASE(4)
     VIA_NTT_I8_CASE(5)

@@ -24,6 +24,12 @@ struct NttTable {
   const u64* ipsi_sh;
   u64 ninv[NTT_MAX_LOGN + 1];
   u64 ninv_sh[NTT_MAX_LOGN + 1];
+  // The same twiddles as exact doubles (q < 2^50), for the double-precision
+  // transforms of ntt_fp.cuh.
+  const double* psi_d;
+  const double* ipsi_d;
+  double qd, qinv;  // q and a rounded 1 / q
+  double ninv_d[NTT_MAX_LOGN + 1];
 };
 
 // Host owner of the device tables of one prime.

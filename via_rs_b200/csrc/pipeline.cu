@@ -21,6 +21,7 @@
 
 #include "first_dim.cuh"
 #include "gadget.cuh"
+#include "ntt_fp.cuh"
 #include "server.cuh"
 
 namespace via {
@@ -869,6 +870,95 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fu
   }
 }
 
+// k_cmux_fused in double precision (ntt_fp.cuh): the same CMux per CTA, the
+// same layouts and digits, with every transform and RGSW product computed as
+// exact integer arithmetic on doubles (FMA two-products and a floating-point
+// quotient estimate) instead of emulated 64-bit integer products. For single
+// primes q < 2^35 and small gadgets: differences of canonical residues are
+// below q; the inverse leaves coefficients within 0.5625 q, made canonical for
+// the digit split; digits below B/2 transform to values below 7 q; each product
+// with an RGSW sample (below q) is reduced to within 0.5625 q, so the 2L
+// products and the input residue sum to less than (1 + 1.125 L) q before the
+// final reduction.
+template <int LOGN>
+__global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fp(const u64* __restrict__ cur,
+                                                                                u64* __restrict__ nxt, KeySel ks,
+                                                                                DevRing R, Gadget g) {
+  constexpr int n = 1 << LOGN;
+  using In0 = NttPhase<LOGN, true, 0>;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  using Fw0 = NttPhase<LOGN, false, 0>;
+  using FwL = NttPhase<LOGN, false, (LOGN + 2) / 3 - 1>;
+  static_assert(In0::STRIDE == 1 && In0::R == 3 && FwL::STRIDE == 1, "contiguous end layouts");
+  __shared__ double ssm[n];
+  const int tid = threadIdx.x;
+  const long o = blockIdx.x;
+  const NttTable& T = R.t[0];
+  const double q = T.qd, qinv = T.qinv;
+  const u64* a = cur + (2 * o) * 2 * n;
+  const u64* b = a + 2 * n;
+  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
+  const int L = g.L;
+  double am[8], ab[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) am[v] = ab[v] = 0.0;
+  for (int p = 0; p < 2; ++p) {  // 0: mask digits (neg_s_m rows), 1: body digits (m rows)
+    double e[8];
+    {
+      const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
+      const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const ulonglong2 x = bv[h], y = av[h];
+        e[2 * h] = __dadd_rn(__ull2double_rn(x.x), -__ull2double_rn(y.x));
+        e[2 * h + 1] = __dadd_rn(__ull2double_rn(x.y), -__ull2double_rn(y.y));
+      }
+    }
+    ntt_inverse_fp<LOGN>(e, tid, T, ssm);
+    __syncthreads();
+#pragma unroll
+    for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
+    __syncthreads();
+    u32 dcur[8];  // scaled coefficients, below B^L < 2^32
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      double c = ssm[swz(Fw0::index(v, tid))];
+      if (c < 0.0) c = __dadd_rn(c, q);
+      dcur[v] = (u32)gadget_scaled_small((u64)__double2ull_rn(c), g);
+    }
+    for (int k = 0; k < L; ++k) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = __ll2double_rn(gadget_next_digit32(dcur[v], g));
+      ntt_forward_fp<LOGN>(e, tid, T, ssm);
+      const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * (p * L + L - 1 - k)) * n + 8 * tid);
+      const ulonglong2* Kb = Km + n / 2;
+#pragma unroll
+      for (int h = 0; h < 4; ++h) {
+        const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
+        am[2 * h] = __dadd_rn(am[2 * h], fp_mulmod(e[2 * h], __ull2double_rn(km.x), q, qinv));
+        am[2 * h + 1] = __dadd_rn(am[2 * h + 1], fp_mulmod(e[2 * h + 1], __ull2double_rn(km.y), q, qinv));
+        ab[2 * h] = __dadd_rn(ab[2 * h], fp_mulmod(e[2 * h], __ull2double_rn(kb.x), q, qinv));
+        ab[2 * h + 1] = __dadd_rn(ab[2 * h + 1], fp_mulmod(e[2 * h + 1], __ull2double_rn(kb.y), q, qinv));
+      }
+    }
+  }
+  ulonglong2* outm = reinterpret_cast<ulonglong2*>(nxt + o * 2 * n + 8 * tid);
+  ulonglong2* outb = outm + n / 2;
+  const ulonglong2* am_in = reinterpret_cast<const ulonglong2*>(a + 8 * tid);
+  const ulonglong2* ab_in = am_in + n / 2;
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const ulonglong2 xm = am_in[h], xb = ab_in[h];
+    ulonglong2 ym, yb;
+    ym.x = __double2ull_rn(fp_canonical(__dadd_rn(__ull2double_rn(xm.x), am[2 * h]), q, qinv));
+    ym.y = __double2ull_rn(fp_canonical(__dadd_rn(__ull2double_rn(xm.y), am[2 * h + 1]), q, qinv));
+    yb.x = __double2ull_rn(fp_canonical(__dadd_rn(__ull2double_rn(xb.x), ab[2 * h]), q, qinv));
+    yb.y = __double2ull_rn(fp_canonical(__dadd_rn(__ull2double_rn(xb.y), ab[2 * h + 1]), q, qinv));
+    outm[h] = ym;
+    outb[h] = yb;
+  }
+}
+
 // The CMux of k_cmux_fused split over a cluster of four CTAs, for tree levels
 // with too few CMuxes to fill the GPU, where one CMux's latency sets the level's
 // time. CTA r of the cluster takes input half p = r & 1 (mask or body),
@@ -952,6 +1042,84 @@ __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
   cluster.sync();
 }
 
+// k_cmux_cluster in double precision (ntt_fp.cuh), with the bounds of
+// k_cmux_fp: each CTA's products are signed residues within 0.5625 q, kept as
+// doubles in shared memory; ranks 0 and 1 add the four partials to in[2o] and
+// reduce once.
+template <int LOGN>
+__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
+    k_cmux_cluster_fp(const u64* __restrict__ cur, u64* __restrict__ nxt, KeySel ks, DevRing R, Gadget g) {
+  namespace cg = cooperative_groups;
+  constexpr int n = 1 << LOGN;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  using Fw0 = NttPhase<LOGN, false, 0>;
+  __shared__ double ssm[n];    // transform exchanges, then the mask partial
+  __shared__ double pbody[n];  // the body partial
+  cg::cluster_group cluster = cg::this_cluster();
+  const int r = (int)cluster.block_rank();
+  const int p = r & 1, k = r >> 1;
+  const int tid = threadIdx.x;
+  const long o = blockIdx.x / 4;
+  const NttTable& T = R.t[0];
+  const double q = T.qd, qinv = T.qinv;
+  const u64* a = cur + (2 * o) * 2 * n;
+  const u64* b = a + 2 * n;
+  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
+  double e[8];
+  {
+    const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
+    const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
+#pragma unroll
+    for (int h = 0; h < 4; ++h) {
+      const ulonglong2 x = bv[h], y = av[h];
+      e[2 * h] = __dadd_rn(__ull2double_rn(x.x), -__ull2double_rn(y.x));
+      e[2 * h + 1] = __dadd_rn(__ull2double_rn(x.y), -__ull2double_rn(y.y));
+    }
+  }
+  ntt_inverse_fp<LOGN>(e, tid, T, ssm);
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
+  __syncthreads();
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    double c = ssm[swz(Fw0::index(v, tid))];
+    if (c < 0.0) c = __dadd_rn(c, q);
+    u32 sc = (u32)gadget_scaled_small((u64)__double2ull_rn(c), g);
+    i64 d = gadget_next_digit32(sc, g);
+    if (k) d = gadget_next_digit32(sc, g);
+    e[v] = __ll2double_rn(d);
+  }
+  ntt_forward_fp<LOGN>(e, tid, T, ssm);
+  const int smp = p * 2 + 1 - k;  // sample L - 1 - k of half p (L = 2)
+  const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * smp) * n + 8 * tid);
+  const ulonglong2* Kb = Km + n / 2;
+  __syncthreads();  // every thread is done with the transform's exchanges in ssm
+#pragma unroll
+  for (int h = 0; h < 4; ++h) {
+    const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
+    const int s0 = 8 * tid + 2 * h;
+    ssm[s0] = fp_mulmod(e[2 * h], __ull2double_rn(km.x), q, qinv);
+    ssm[s0 + 1] = fp_mulmod(e[2 * h + 1], __ull2double_rn(km.y), q, qinv);
+    pbody[s0] = fp_mulmod(e[2 * h], __ull2double_rn(kb.x), q, qinv);
+    pbody[s0 + 1] = fp_mulmod(e[2 * h + 1], __ull2double_rn(kb.y), q, qinv);
+  }
+  cluster.sync();
+  if (r < 2) {  // rank 0: the output mask, rank 1: the output body
+    double* parts[4];
+#pragma unroll
+    for (int rr = 0; rr < 4; ++rr) parts[rr] = cluster.map_shared_rank(r == 0 ? ssm : pbody, rr);
+    u64* out = nxt + o * 2 * n + (long)r * n;
+    for (int x = tid; x < n; x += blockDim.x) {
+      double acc = __ull2double_rn(a[(long)r * n + x]);
+#pragma unroll
+      for (int rr = 0; rr < 4; ++rr) acc = __dadd_rn(acc, parts[rr][x]);
+      out[x] = __double2ull_rn(fp_canonical(acc, q, qinv));
+    }
+  }
+  cluster.sync();
+}
+
 // CMux level o < count: fused kernel when the ring has one NTT limb of a
 // supported degree and a small gadget, else diff -> external product -> add.
 static bool cmux_fused_ok(const DevRing& R, const Gadget& g) {
@@ -965,18 +1133,18 @@ static void cmux_fused(const DevRing& R, const Gadget& g, const u64* cur, u64* n
   // four-CTA cluster to cut its latency.
   if (count <= 64 && g.L == 2 && R.n <= 2048) {
     switch (R.n) {
-      case 2048: k_cmux_cluster<11><<<(unsigned)(4 * count), 256, 0, st>>>(cur, nxt, ks, R, g); break;
-      case 1024: k_cmux_cluster<10><<<(unsigned)(4 * count), 128, 0, st>>>(cur, nxt, ks, R, g); break;
-      default: k_cmux_cluster<9><<<(unsigned)(4 * count), 64, 0, st>>>(cur, nxt, ks, R, g); break;
+      case 2048: k_cmux_cluster_fp<11><<<(unsigned)(4 * count), 256, 0, st>>>(cur, nxt, ks, R, g); break;
+      case 1024: k_cmux_cluster_fp<10><<<(unsigned)(4 * count), 128, 0, st>>>(cur, nxt, ks, R, g); break;
+      default: k_cmux_cluster_fp<9><<<(unsigned)(4 * count), 64, 0, st>>>(cur, nxt, ks, R, g); break;
     }
     VIA_LAUNCHED();
     return;
   }
   switch (R.n) {
-    case 4096: k_cmux_fused<12><<<(unsigned)count, 512, 0, st>>>(cur, nxt, ks, R, g); break;
-    case 2048: k_cmux_fused<11><<<(unsigned)count, 256, 0, st>>>(cur, nxt, ks, R, g); break;
-    case 1024: k_cmux_fused<10><<<(unsigned)count, 128, 0, st>>>(cur, nxt, ks, R, g); break;
-    default: k_cmux_fused<9><<<(unsigned)count, 64, 0, st>>>(cur, nxt, ks, R, g); break;
+    case 4096: k_cmux_fp<12><<<(unsigned)count, 512, 0, st>>>(cur, nxt, ks, R, g); break;
+    case 2048: k_cmux_fp<11><<<(unsigned)count, 256, 0, st>>>(cur, nxt, ks, R, g); break;
+    case 1024: k_cmux_fp<10><<<(unsigned)count, 128, 0, st>>>(cur, nxt, ks, R, g); break;
+    default: k_cmux_fp<9><<<(unsigned)count, 64, 0, st>>>(cur, nxt, ks, R, g); break;
   }
   VIA_LAUNCHED();
 }
