@@ -209,40 +209,99 @@ __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_reg_i8(const int8_t* __
                                          din + (active ? seg / nl : 0) * n);
 }
 
-// k_ntt_reg_i8 in double precision (ntt_fp.cuh): the digits (|d| <= 127) are
-// transformed as exact integer doubles; the outputs, within 0.5625 LOGN q + 127
-// of zero, are offset by OFF q (OFF = ceil(0.5625 LOGN) + 1) to a nonnegative
-// residue below (1.125 LOGN + 3) q <= (1 + 2 LOGN) q, the bound of the integer
-// kernel's lazy outputs, and stored as u64. Primes below 2^44 (values stay far
-// below 2^48).
-template <int LOGN, int P>
-__device__ __forceinline__ void ntt_fp_phases_i8(double (&e)[8], int tid, const NttTable& T, u64* g, double* sm,
-                                                 int sbase, bool active) {
-  using Ph = NttPhaseFp<LOGN, false, P>;
-  using Ix = NttPhase<LOGN, false, P>;
+// ---------------------------------------------------------------------------
+// The register-resident transforms in double precision (ntt_fp.cuh), for primes
+// below 2^44: the same layouts and phases as ntt_phases, exact integer
+// arithmetic on doubles. Inputs are residues below 2^47 (larger values are
+// reduced first); outputs:
+//  * forward: canonical residues, or (LAZY) nonnegative residues below
+//    (1.125 LOGN + 3) q <= (1 + 2 LOGN) q, the integer kernel's lazy bound;
+//    forward values stay within |input| + 0.5625 LOGN q of zero;
+//  * inverse: canonical residues. Inverse values at most double per stage; for
+//    q above 2^35 every phase boundary first reduces them to within q/2, so a
+//    phase of three stages ends below 4 q and every product stays exact.
+// I8: the input is a polynomial of signed 8-bit digits.
+// ---------------------------------------------------------------------------
+// DOUT: the (forward, lazy) outputs are stored as the signed doubles themselves.
+template <int LOGN, bool INV, int P, bool LAZY, bool I8, bool DOUT = false>
+__device__ __forceinline__ void ntt_fp_phases(double (&e)[8], int tid, const NttTable& T, u64* g, double* sm,
+                                              int sbase, bool active, const int8_t* gin) {
+  using Ph = NttPhaseFp<LOGN, INV, P>;
+  using Ix = NttPhase<LOGN, INV, P>;
   constexpr int NPH = (LOGN + 2) / 3;
-  if (P > 0) {
+  const double q = T.qd, qinv = T.qinv;
+  if constexpr (P == 0) {
+    if constexpr (I8) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = active ? (double)gin[Ix::index(v, tid)] : 0.0;
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) {
+        u64 x = active ? g[Ix::index(v, tid)] : 0;
+        if (x >= (1ull << 47)) x %= T.q;
+        e[v] = __ull2double_rn(x);
+      }
+    }
+  } else {
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) e[v] = sm[swz(sbase + Ix::index(v, tid))];
+    if (INV && q > 34359738368.0) {  // q > 2^35: restart the inverse's growth at q/2
+#pragma unroll
+      for (int v = 0; v < 8; ++v)
+        e[v] = __fma_rn(-__dadd_rn(__fma_rn(e[v], qinv, FP_ROUND), -FP_ROUND), q, e[v]);
+    }
   }
   Ph::run(e, tid, T);
   if constexpr (P == NPH - 1) {
-    constexpr int OFF = (9 * LOGN + 15) / 16 + 1;  // ceil(0.5625 LOGN) + 1
-    const double off = (double)OFF * T.qd;
+    if constexpr (INV) {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = fp_canonical(fp_mulmod(e[v], T.ninv_d[LOGN], q, qinv), q, qinv);
+    } else if constexpr (DOUT) {
+      if (active) {
+        double* gd = reinterpret_cast<double*>(g);
+#pragma unroll
+        for (int v = 0; v < 8; ++v) gd[Ix::index(v, tid)] = e[v];
+      }
+      return;
+    } else if constexpr (LAZY) {
+      constexpr int OFF = (9 * LOGN + 15) / 16 + 1;  // ceil(0.5625 LOGN) + 1
+      const double off = (double)OFF * q;
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = __dadd_rn(e[v], off);
+    } else {
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = fp_canonical(e[v], q, qinv);
+    }
     if (active) {
 #pragma unroll
-      for (int v = 0; v < 8; ++v) g[Ix::index(v, tid)] = __double2ull_rn(__dadd_rn(e[v], off));
+      for (int v = 0; v < 8; ++v) g[Ix::index(v, tid)] = __double2ull_rn(e[v]);
     }
   } else {
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) sm[swz(sbase + Ix::index(v, tid))] = e[v];
-    ntt_fp_phases_i8<LOGN, P + 1>(e, tid, T, g, sm, sbase, active);
+    ntt_fp_phases<LOGN, INV, P + 1, LAZY, false, DOUT>(e, tid, T, g, sm, sbase, active, nullptr);
   }
 }
 
-template <int LOGN>
+template <int LOGN, bool INV, bool LAZY = false>
+__global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_fp(u64* __restrict__ data, int nl, long segments,
+                                                            NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  constexpr int TPS = n / 8;
+  constexpr int SPC = ntt_cta<LOGN>() / TPS;
+  __shared__ double sm[ntt_cta<LOGN>() * 8];
+  const int seg_local = threadIdx.x / TPS;
+  const int tid = threadIdx.x % TPS;
+  const long seg = (long)blockIdx.x * SPC + seg_local;
+  const bool active = seg < segments;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  double e[8];
+  ntt_fp_phases<LOGN, INV, 0, LAZY, false>(e, tid, T, data + seg * n, sm, seg_local * n, active, nullptr);
+}
+
+template <int LOGN, bool DOUT = false>
 __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_fp_i8(const int8_t* __restrict__ din, u64* __restrict__ out,
                                                                int nl, long segments, NttTable t0, NttTable t1) {
   constexpr int n = 1 << LOGN;
@@ -254,12 +313,41 @@ __global__ void __launch_bounds__(ntt_cta<LOGN>()) k_ntt_fp_i8(const int8_t* __r
   const long seg = (long)blockIdx.x * SPC + seg_local;
   const bool active = seg < segments;
   const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
-  const int8_t* gin = din + (active ? seg / nl : 0) * n;
   double e[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) e[v] = active ? (double)gin[NttPhase<LOGN, false, 0>::index(v, tid)] : 0.0;
-  ntt_fp_phases_i8<LOGN, 0>(e, tid, T, out + seg * n, sm, seg_local * n, active);
+  ntt_fp_phases<LOGN, false, 0, true, true, DOUT>(e, tid, T, out + seg * n, sm, seg_local * n, active,
+                                                  din + (active ? seg / nl : 0) * n);
 }
+
+// n = 2 and 4 on 8-bit digits, double outputs: one thread per segment.
+template <int LOGN>
+__global__ void k_ntt_tiny_i8_fp(const int8_t* __restrict__ din, double* __restrict__ out, int nl, long segments,
+                                 NttTable t0, NttTable t1) {
+  constexpr int n = 1 << LOGN;
+  long seg = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (seg >= segments) return;
+  const NttTable& T = (nl == 2 && (seg & 1)) ? t1 : t0;
+  double a[n];
+  const int8_t* gi = din + (seg / nl) * n;
+#pragma unroll
+  for (int i = 0; i < n; ++i) a[i] = (double)gi[i];
+#pragma unroll
+  for (int len = n / 2, m = 1; len >= 1; len >>= 1, m <<= 1)
+#pragma unroll
+    for (int x = 0; x < n; ++x) {
+      if ((x / len) & 1) continue;
+      const int grp = x / (2 * len);
+      const double t = fp_mulmod(a[x + len], T.psi_d[m + grp], T.qd, T.qinv);
+      const double u = a[x];
+      a[x] = __dadd_rn(u, t);
+      a[x + len] = __dadd_rn(u, -t);
+    }
+  double* g = out + seg * n;
+#pragma unroll
+  for (int i = 0; i < n; ++i) g[i] = a[i];
+}
+
+// The double-precision kernels serve primes below 2^44 (exact products, ntt_fp.cuh).
+static bool fp_ok(const NttTable& t0, const NttTable& t1) { return t0.q < (1ull << 44) && t1.q < (1ull << 44); }
 
 // n = 2 and 4 on 8-bit digits: one thread per segment.
 template <int LOGN>
@@ -348,9 +436,15 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
   const int cta = std::max(NTT_THREADS, n / 8);
   long spc = cta / (n / 8);
   unsigned blocks = (unsigned)((segments + spc - 1) / spc);
+  const bool fp = fp_ok(t0, t1);
   switch (logn) {
-#define VIA_NTT_CASE(LG) \
-  case LG: k_ntt_reg<LG, INV, LAZY><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1); break;
+#define VIA_NTT_CASE(LG)                                                              \
+  case LG:                                                                           \
+    if (fp)                                                                          \
+      k_ntt_fp<LG, INV, LAZY><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1);   \
+    else                                                                             \
+      k_ntt_reg<LG, INV, LAZY><<<blocks, cta, 0, st>>>(data, nl, segments, t0, t1);  \
+    break;
     VIA_NTT_CASE(3)
     VIA_NTT_CASE(4)
     VIA_NTT_CASE(5)
@@ -392,8 +486,7 @@ void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segmen
   const int cta = std::max(NTT_THREADS, n / 8);
   const long spc = cta / (n / 8);
   const unsigned blocks = (unsigned)((segments + spc - 1) / spc);
-  // Double precision when both primes are below 2^44 (exact products, see ntt_fp.cuh).
-  const bool fp = t0.q < (1ull << 44) && t1.q < (1ull << 44);
+  const bool fp = fp_ok(t0, t1);
   switch (logn) {
 #define VIA_NTT_I8_CASE(LG)                                                            \
   case LG:                                                                             \
@@ -416,5 +509,42 @@ void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segmen
   }
   VIA_LAUNCHED();
 }
+
+void ntt_forward_i8_fp(const int8_t* din, double* out, int n, int nl, long segments, const NttTable& t0,
+                       const NttTable& t1, cudaStream_t st) {
+  if (segments <= 0) return;
+  const int logn = __builtin_ctz((unsigned)n);
+  if (n < 2 || (n & (n - 1)) || logn > 12) throw CudaError(100, "ntt: degree must be a power of two in [2, 4096]");
+  if (!fp_ok(t0, t1)) throw CudaError(100, "ntt: double-precision outputs need primes below 2^44");
+  u64* o = reinterpret_cast<u64*>(out);
+  if (logn <= 2) {
+    const unsigned blocks = (unsigned)((segments + 127) / 128);
+    if (logn == 1) k_ntt_tiny_i8_fp<1><<<blocks, 128, 0, st>>>(din, out, nl, segments, t0, t1);
+    else k_ntt_tiny_i8_fp<2><<<blocks, 128, 0, st>>>(din, out, nl, segments, t0, t1);
+    VIA_LAUNCHED();
+    return;
+  }
+  const int cta = std::max(NTT_THREADS, n / 8);
+  const long spc = cta / (n / 8);
+  const unsigned blocks = (unsigned)((segments + spc - 1) / spc);
+  switch (logn) {
+#define VIA_NTT_I8D_CASE(LG) \
+  case LG: k_ntt_fp_i8<LG, true><<<blocks, cta, 0, st>>>(din, o, nl, segments, t0, t1); break;
+    VIA_NTT_I8D_CASE(3)
+    VIA_NTT_I8D_CASE(4)
+    VIA_NTT_I8D_CASE(5)
+    VIA_NTT_I8D_CASE(6)
+    VIA_NTT_I8D_CASE(7)
+    VIA_NTT_I8D_CASE(8)
+    VIA_NTT_I8D_CASE(9)
+    VIA_NTT_I8D_CASE(10)
+    VIA_NTT_I8D_CASE(11)
+    VIA_NTT_I8D_CASE(12)
+#undef VIA_NTT_I8D_CASE
+  }
+  VIA_LAUNCHED();
+}
+
+bool ntt_fp_ok(const NttTable& t0, const NttTable& t1) { return fp_ok(t0, t1); }
 
 }  // namespace via

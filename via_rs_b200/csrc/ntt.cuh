@@ -200,5 +200,11 @@ void ntt_forward_lazy(u64* data, int n, int nl, long segments, const NttTable& t
 // polynomial s / nl) reads din + (s / nl) * n and writes out + s * n.
 void ntt_forward_i8_lazy(const int8_t* din, u64* out, int n, int nl, long segments, const NttTable& t0,
                          const NttTable& t1, cudaStream_t st);
+// The same with signed double outputs (within 0.5625 log2(n) q + 127 of zero,
+// exact integers), for the double-precision multiply-accumulates; primes below 2^44.
+void ntt_forward_i8_fp(const int8_t* din, double* out, int n, int nl, long segments, const NttTable& t0,
+                       const NttTable& t1, cudaStream_t st);
+// Whether the double-precision transforms serve these primes (both below 2^44).
+bool ntt_fp_ok(const NttTable& t0, const NttTable& t1);
 
 }  // namespace via

@@ -338,6 +338,57 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
   }
 }
 
+// k_cascade_mac in double precision (ntt_fp.cuh): D holds the digits' signed
+// double transforms (ntt_forward_i8_fp, within 7 q of zero), keys the cascade
+// key as exact doubles (below q). Every product is reduced to within 0.5625 q,
+// so a mask's 2 L products stay below 1.125 L q; the body partial is brought
+// back within q/2 after each output mask's 2 L products. Outputs as k_cascade_mac.
+__global__ void __launch_bounds__(256) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
+                                                        int R, int n_in, int L, int TT, int JB, DevRing Rg,
+                                                        u64* __restrict__ mask_out, u64* __restrict__ bsum,
+                                                        u64* __restrict__ bpart) {
+  __shared__ u64 part[256];
+  const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
+  const int JJ = 256 / TT;
+  const int jb = blockIdx.x % JB;
+  const int tl = threadIdx.x % TT, jl = threadIdx.x / TT;
+  const int t = (blockIdx.x / JB) * TT + tl;
+  const int l = blockIdx.y;
+  const long lwe = blockIdx.z;
+  const DevMod& m = Rg.m[l];
+  const double q = Rg.t[l].qd, qinv = Rg.t[l].qinv;
+  const long dper = (long)nl * n_in, kper = (long)nl * n_out;
+  const double* Dw = D + lwe * R * L * dper + (long)l * n_in + (t >> 1);
+  const double* Kl = keys + (long)l * n_out + t;
+  double ab = 0.0;
+  for (int j = jl + jb * JJ; j < half; j += JJ * JB) {
+    double am = 0.0;
+    const double* d0 = Dw + (long)j * L * dper;
+    const double* d1 = Dw + (long)(j + half) * L * dper;
+    const double* k0 = Kl + (long)j * L * 2 * kper;
+    const double* k1 = Kl + (long)(j + half) * L * 2 * kper;
+#pragma unroll 3
+    for (int s = 0; s < L; ++s) {
+      const double a = d0[s * dper], b = d1[s * dper];
+      am = __dadd_rn(am, __dadd_rn(fp_mulmod(a, k0[(2 * s) * kper], q, qinv), fp_mulmod(b, k1[(2 * s) * kper], q, qinv)));
+      ab = __dadd_rn(ab, __dadd_rn(fp_mulmod(a, k0[(2 * s + 1) * kper], q, qinv),
+                                   fp_mulmod(b, k1[(2 * s + 1) * kper], q, qinv)));
+    }
+    mask_out[((lwe * half + j) * nl + l) * n_out + t] = negmod(__double2ull_rn(fp_canonical(am, q, qinv)), m.q);
+    ab = __fma_rn(-__dadd_rn(__fma_rn(ab, qinv, FP_ROUND), -FP_ROUND), q, ab);  // back within q/2
+  }
+  part[threadIdx.x] = __double2ull_rn(fp_canonical(ab, q, qinv));
+  __syncthreads();
+  if (jl == 0) {
+    u64 acc = part[tl];
+    for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
+    if (JB == 1)
+      bsum[(lwe * nl + l) * n_out + t] = acc;
+    else
+      bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
+  }
+}
+
 // bsum[lwe][l][t] = sum over jb of bpart[lwe][jb][l][t] (mod q_l).
 __global__ void k_cascade_bsum(const u64* __restrict__ bpart, int JB, int nl, int n_out, long nlwe, DevRing Rg,
                                u64* __restrict__ bsum) {
@@ -698,10 +749,14 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
     const long polys = nlwe * rank_in;
     if (R.ntt) {
       // Digits at the input degree; see k_cascade_mac for the repeated slots.
+      const bool fp_mac = dig8 && n_in > 1 && s.cascade_eval_d.p;
       if (dig8 && n_in > 1) {
         k_decompose_i8<<<blocks(polys * n_in, 128), 128, 0, st>>>(mi, n_in, polys, R, w.g_ck, dig8);
         VIA_LAUNCHED();
-        ntt_forward_i8_lazy(dig8, digits, n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
+        if (fp_mac)
+          ntt_forward_i8_fp(dig8, reinterpret_cast<double*>(digits), n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
+        else
+          ntt_forward_i8_lazy(dig8, digits, n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
       } else {
         decompose(R, w.g_ck, mi, n_in, 1, polys, digits, st);
         if (n_in > 1) digits_to_eval(R, digits, n_in, polys * L * nl, st);
@@ -714,8 +769,13 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
       int JB = 1;
       while (JB * 2 <= iters && base * JB * 2 <= CASCADE_SPLIT_BLOCKS) JB *= 2;
       dim3 grid((unsigned)(n_out / tt * JB), (unsigned)nl, (unsigned)nlwe);
-      k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
-                                          bsum, bpart);
+      if (fp_mac)
+        k_cascade_mac_fp<<<grid, 256, 0, st>>>(reinterpret_cast<const double*>(digits),
+                                               reinterpret_cast<const double*>(s.cascade_eval_d.p) + k * step_len,
+                                               rank_in, n_in, L, tt, JB, R, mo, bsum, bpart);
+      else
+        k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
+                                            bsum, bpart);
       VIA_LAUNCHED();
       if (JB > 1) {
         k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bpart, JB, nl, n_out, nlwe, R, bsum);

@@ -186,6 +186,11 @@ Server::~Server() {
   if (stream) cudaStreamDestroy(stream);
 }
 
+__global__ void k_u64_to_f64(const u64* __restrict__ in, double* __restrict__ out, long count) {
+  const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (gid < count) out[gid] = __ull2double_rn(in[gid]);
+}
+
 static void transform_keys(Server& s) {
   const via_params& p = s.prm;
   // Cascade: step k (output degree 2^k) has 2*n1*L_CK*2*nl residues.
@@ -195,6 +200,13 @@ static void transform_keys(Server& s) {
       ntt_forward(s.cascade_eval.p + (k - 1) * step, nout, s.r1.nl, (long)(step / nout), s.r1.t[0], s.r1.t[1],
                   s.stream);
     ntt_forward(s.conv_eval.p, p.n1, s.r1.nl, (long)p.l_ck * 2 * s.r1.nl, s.r1.t[0], s.r1.t[1], s.stream);
+    if (ntt_fp_ok(s.r1.t[0], s.r1.t[1]) && p.ck_base <= 255) {  // the 8-bit digit path's double-precision MAC
+      s.cascade_eval_d.alloc(s.cascade_eval.n);
+      const long count = (long)s.cascade_eval.n;
+      k_u64_to_f64<<<(unsigned)((count + 255) / 256), 256, 0, s.stream>>>(
+          s.cascade_eval.p, reinterpret_cast<double*>(s.cascade_eval_d.p), count);
+      VIA_LAUNCHED();
+    }
   }
   if (s.r3.ntt)
     ntt_forward(s.rsk_eval.p, p.n2, 1, (long)(p.n1 / p.n2) * p.l_rsk * 2, s.r3.t[0], s.r3.t[1], s.stream);

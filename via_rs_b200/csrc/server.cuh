@@ -61,6 +61,7 @@ struct Server {
   DevBuf fd_err;  // one device word the scan sets when a bounded wait runs out
   // Eval-form keys (crates/via-server/src/prepared_keys.rs:69-79).
   DevBuf cascade_eval;  // include/via_gpu.h cascade layout, each segment transformed
+  DevBuf cascade_eval_d;  // the same residues as exact doubles (q1 primes below 2^44), for the double-precision MAC
   DevBuf conv_eval;     // L_CK samples at (q1, n1)
   DevBuf rsk_eval;      // d RLevs at (q3, n2)
   // VIA-B repack keys (n_rec < n2): the cascade steps of output degree 2 n_rec .. n1,
