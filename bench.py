@@ -89,6 +89,16 @@ def load_peaks():
     return 6650.0, "fallback"
 
 
+def load_tensor_peak():
+    """Dense bf16 tensor TFLOP/s (burst), measured when MEASURED_PEAKS.json holds it."""
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        d = json.loads(p.read_text())
+        if "bf16_tflops" in d:
+            return float(d["bf16_tflops"]), "measured"
+    return 1590.0, "fallback"
+
+
 # ---------------------------------------------------------------------------
 # Synthetic inputs (seeded). Key and query residues are uniform: the answer's
 # cost does not depend on their values; correctness is covered by the tests.
@@ -779,6 +789,25 @@ def gpu_arm(args, prm):
     scan_bytes = db_bytes + sel.numel() * 8 + out.numel() * 8
     peak, peak_kind = load_peaks()
     achieved = scan_bytes / scan_s / 1e9
+
+    # ---- the batched scan as a tensor-core contraction: B queries' selections
+    # against the byte planes, 25 byte-product GEMMs per eval slot (kind::i8).
+    # Its time is the autotuner's live CUDA-event measurement of the kept tile
+    # (three timed scans on preallocated buffers).
+    roofline_batched = None
+    tuned_b = next((e for e in tuning if e["batch"] == args.batch), None) if args.batch > 1 else None
+    if tuned_b:
+        B = args.batch
+        bscan_s = tuned_b["ms"] / 1e3
+        macs = 25.0 * prm.n1 * prm.num_rows * prm.num_cols * 2 * B  # byte products, all 25 limb pairs
+        tpeak, tpeak_kind = load_tensor_peak()
+        i8_peak = 2.0 * tpeak  # dense int8 = 2x dense bf16 on this tensor core
+        achieved_tops = 2.0 * macs / bscan_s / 1e12
+        roofline_batched = {"bound": "tensor", "kernel": f"k_fd_split + k_fd_tc, {B} queries (tcgen05 kind::i8)",
+                            "achieved": achieved_tops, "peak": i8_peak, "unit": "TOP/s (int8)",
+                            "frac": achieved_tops / i8_peak, "peak_kind": f"2x {tpeak_kind} bf16 TFLOP/s",
+                            "launch_ms": bscan_s * 1e3, "tile": tuned_b["tile"], "int8_ops": 2.0 * macs,
+                            "db_gbs": db_bytes / bscan_s / 1e9}
     server.close()
     del server, d_q, sel, out
     torch.cuda.empty_cache()
@@ -813,6 +842,7 @@ def gpu_arm(args, prm):
                          "traffic": (SCAN_READ_BYTES_PER_CELL * prm.num_rows * prm.num_cols
                                      + SCAN_WRITE_BYTES_PER_COLUMN * prm.num_cols),
                          "launch_ms": scan_s * 1e3, "algorithmic_bytes": scan_bytes},
+            "roofline_batched": roofline_batched,
             "e2e": {"value": e2e_value, "unit": "answers/s", "h2d_bytes_per_step": int(query.nbytes),
                     "d2h_bytes_per_step": int(2 * prm.n2 * 8)},
             "autotune": tuning,
