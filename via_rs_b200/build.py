@@ -37,7 +37,10 @@ def build(force: bool = False, verbose: bool = False) -> pathlib.Path:
     procs = []
     for src in sources():
         obj = build_dir / (src.stem + ".o")
-        cmd = [NVCC, *ARCH, *FLAGS, "-dc", "-c", str(src), "-o", str(obj)]
+        # Whole-program compilation per file (no relocatable device code): no
+        # kernel calls device code of another file, and ptxas then allocates
+        # far fewer registers for the transform and multiply-accumulate kernels.
+        cmd = [NVCC, *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd))
         procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))
