@@ -436,9 +436,7 @@ static void launch(u64* data, int n, int nl, long segments, const NttTable& t0, 
   const int cta = std::max(NTT_THREADS, n / 8);
   long spc = cta / (n / 8);
   unsigned blocks = (unsigned)((segments + spc - 1) / spc);
-  // The double-precision kernels measured faster than the integer ones for the
-  // inverse only; forward transforms keep the lazy Shoup butterflies.
-  const bool fp = INV && fp_ok(t0, t1);
+  const bool fp = fp_ok(t0, t1);
   switch (logn) {
 #define VIA_NTT_CASE(LG)                                                              \
   case LG:                                                                           \

@@ -343,7 +343,8 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
 // key as exact doubles (below q). Every product is reduced to within 0.5625 q,
 // so a mask's 2 L products stay below 1.125 L q; the body partial is brought
 // back within q/2 after each output mask's 2 L products. Outputs as k_cascade_mac.
-__global__ void __launch_bounds__(256) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
+// Two CTAs per SM leave room for nine digits' loads in flight per thread.
+__global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
                                                         int R, int n_in, int L, int TT, int JB, DevRing Rg,
                                                         u64* __restrict__ mask_out, u64* __restrict__ bsum,
                                                         u64* __restrict__ bpart) {
@@ -367,7 +368,7 @@ __global__ void __launch_bounds__(256) k_cascade_mac_fp(const double* __restrict
     const double* d1 = Dw + (long)(j + half) * L * dper;
     const double* k0 = Kl + (long)j * L * 2 * kper;
     const double* k1 = Kl + (long)(j + half) * L * 2 * kper;
-#pragma unroll 3
+#pragma unroll 9
     for (int s = 0; s < L; ++s) {
       const double a = d0[s * dper], b = d1[s * dper];
       am = __dadd_rn(am, __dadd_rn(fp_mulmod(a, k0[(2 * s) * kper], q, qinv), fp_mulmod(b, k1[(2 * s) * kper], q, qinv)));
