@@ -202,6 +202,91 @@ __global__ void k_dmux_combine(u64* out, const u64* in, const u64* ext, long cou
   out[(2 * j + 1) * per + rem] = e;
 }
 
+// One DMux tree level in a single kernel (mux.rs:129-137, 222-251; the external
+// product rgsw.rs:108-121 with the coefficient-form gadget product,
+// rlev.rs:193-222), in double precision (ntt_fp.cuh). CTA (o, l) computes limb l
+// of ext[o] = bit (x) in[o] and writes out[2o] = in[o] - ext, out[2o+1] = ext:
+// the gadget digits (L = 2) of the mask and body coefficients (both limbs read,
+// one CRT scaling per coefficient, digits kept in shared memory), forward
+// transforms of the four digit polynomials at prime l, products with the RGSW
+// samples (each within 0.5625 q; digit k of input half h with sample
+// h L + L - 1 - k), and inverse transforms of the two sums (below 2.25 q).
+// Buffers: [ct][2][nl][n], RGSW [2L][2][nl][n] eval at q1; nl = 2 primes below 2^44.
+template <int LOGN>
+__global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_dmux_fp(u64* __restrict__ out, const u64* __restrict__ in,
+                                                                  KeySel ks, DevRing R, Gadget g) {
+  constexpr int n = 1 << LOGN;
+  constexpr int L = 2;
+  constexpr int nl = 2;
+  using Fw0 = NttPhase<LOGN, false, 0>;
+  using FwL = NttPhase<LOGN, false, (LOGN + 2) / 3 - 1>;
+  using In0 = NttPhase<LOGN, true, 0>;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  static_assert(In0::STRIDE == 1 && In0::R == 3 && FwL::STRIDE == 1, "contiguous end layouts");
+  __shared__ double ssm[n];
+  __shared__ int dgs[L][n];  // one half's digits; each thread reads back only its own slots
+  const int tid = threadIdx.x;
+  const long o = blockIdx.x;
+  const int l = blockIdx.y;
+  const NttTable& T = R.t[l];
+  const double q = T.qd, qinv = T.qinv;
+  const u64* ct = in + o * 2 * nl * n;
+  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
+  double am[8], ab[8];
+#pragma unroll
+  for (int v = 0; v < 8; ++v) am[v] = ab[v] = 0.0;
+  for (int h = 0; h < 2; ++h) {  // 0: mask digits (neg_s_m rows), 1: body digits (m rows)
+#pragma unroll
+    for (int v = 0; v < 8; ++v) {
+      const int x = Fw0::index(v, tid);
+      const u64 a0 = ct[(long)h * nl * n + x], a1 = ct[(long)h * nl * n + n + x];
+      for_each_digit(gadget_scaled(a0, a1, R, g), g, [&](int k, i64 d) { dgs[k][x] = (int)d; });
+    }
+#pragma unroll 1
+    for (int k = 0; k < L; ++k) {
+      double e[8];
+#pragma unroll
+      for (int v = 0; v < 8; ++v) e[v] = (double)dgs[k][Fw0::index(v, tid)];
+      ntt_forward_fp<LOGN>(e, tid, T, ssm);
+      const int smp = h * L + L - 1 - k;
+      const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + ((long)(2 * smp) * nl + l) * n + 8 * tid);
+      const ulonglong2* Kb = reinterpret_cast<const ulonglong2*>(K + ((long)(2 * smp + 1) * nl + l) * n + 8 * tid);
+#pragma unroll
+      for (int c = 0; c < 4; ++c) {
+        const ulonglong2 km = __ldg(Km + c), kb = __ldg(Kb + c);
+        am[2 * c] = __dadd_rn(am[2 * c], fp_mulmod(e[2 * c], __ull2double_rn(km.x), q, qinv));
+        am[2 * c + 1] = __dadd_rn(am[2 * c + 1], fp_mulmod(e[2 * c + 1], __ull2double_rn(km.y), q, qinv));
+        ab[2 * c] = __dadd_rn(ab[2 * c], fp_mulmod(e[2 * c], __ull2double_rn(kb.x), q, qinv));
+        ab[2 * c + 1] = __dadd_rn(ab[2 * c + 1], fp_mulmod(e[2 * c + 1], __ull2double_rn(kb.y), q, qinv));
+      }
+    }
+  }
+  const u64 qi = R.m[l].q;
+  u64* o0 = out + (2 * o) * 2 * nl * n;
+  u64* o1 = o0 + 2 * nl * n;
+  ntt_inverse_fp<LOGN>(am, tid, T, ssm);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {  // ext mask
+    const long at = (long)l * n + InL::index(v, tid);
+    const u64 ext = __double2ull_rn(fp_canonical(am[v], q, qinv));
+    o0[at] = submod(ct[at], ext, qi);
+    o1[at] = ext;
+  }
+  __syncthreads();  // the body's transform reuses the exchange area
+  ntt_inverse_fp<LOGN>(ab, tid, T, ssm);
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {  // ext body
+    const long at = (long)(nl + l) * n + InL::index(v, tid);
+    const u64 ext = __double2ull_rn(fp_canonical(ab[v], q, qinv));
+    o0[at] = submod(ct[at], ext, qi);
+    o1[at] = ext;
+  }
+}
+
+static bool dmux_fp_ok(const DevRing& R, const Gadget& g) {
+  return R.ntt && R.nl == 2 && g.L == 2 && ntt_fp_ok(R.t[0], R.t[1]) && R.n == 2048;
+}
+
 // Modulus switch (prim/switching/kernels/mod_switch.rs:59-61):
 // c' = floor((c * q_dst + floor(q_src/2)) / q_src) mod q_dst, c the canonical value.
 __global__ void k_mod_switch(const u64* __restrict__ in, DevRing S, u64* __restrict__ out, DevMod dst, long ncoef,
@@ -1361,6 +1446,15 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
     for (int i = 0; i < nd; ++i) {
       const long active = 1L << i;  // per query
       KeySel bit{w.rgsw_q1.p + i * rgsw1, active, B, nd * rgsw1};
+      // The fused level kernel is latency-bound at about 70 us for up to a wave of
+      // products (148 SMs x 2 CTAs, two per product); smaller levels keep the
+      // separate, wider kernels (about 40 us a level).
+      if (dmux_fp_ok(s.r1, w.g_dmux) && B * active >= 256) {
+        k_dmux_fp<11><<<dim3((unsigned)(B * active), 2), 256, 0, st>>>(out, in, bit, s.r1, w.g_dmux);
+        VIA_LAUNCHED();
+        std::swap(in, out);
+        continue;
+      }
       external_products(s.r1, w.g_dmux, bit, in, B * active, w.dm_digits.p, w.dm_ext.p, true, st);
       k_dmux_combine<<<blocks(B * active * 2 * nl * n1), 256, 0, st>>>(out, in, w.dm_ext.p, B * active, n1, nl, s.r1);
       VIA_LAUNCHED();
