@@ -110,10 +110,10 @@ __device__ __forceinline__ void ntt_forward_fp(double (&e)[8], int tid, const Nt
 
 // Inverse transform (then the n^-1 scaling) of a segment held in the layout
 // NttPhase<LOGN, true, 0>::index, inputs below 4 q in magnitude; leaves signed
-// coefficients, |x| <= 0.5625 q, in the layout of the last inverse phase. For
-// q above 2^35 every phase boundary first brings the values back within q/2
-// (a phase of three stages then stays below 32 q).
-template <int LOGN, int P = 0>
+// coefficients, |x| <= 0.5625 q, in the layout of the last inverse phase. With
+// REDUCE (needed for q above 2^35) every phase boundary first brings the values
+// back within q/2, so a phase of three stages stays below 32 q.
+template <int LOGN, int P = 0, bool REDUCE = false>
 __device__ __forceinline__ void ntt_inverse_fp(double (&e)[8], int tid, const NttTable& T, double* ssm) {
   using Ph = NttPhaseFp<LOGN, true, P>;
   constexpr int NPH = (LOGN + 2) / 3;
@@ -126,12 +126,12 @@ __device__ __forceinline__ void ntt_inverse_fp(double (&e)[8], int tid, const Nt
     __syncthreads();
 #pragma unroll
     for (int v = 0; v < 8; ++v) e[v] = ssm[swz(Nx::index(v, tid))];
-    if (T.qd > 34359738368.0) {  // q > 2^35
+    if constexpr (REDUCE) {
 #pragma unroll
       for (int v = 0; v < 8; ++v)
         e[v] = __fma_rn(-__dadd_rn(__fma_rn(e[v], T.qinv, FP_ROUND), -FP_ROUND), T.qd, e[v]);
     }
-    ntt_inverse_fp<LOGN, P + 1>(e, tid, T, ssm);
+    ntt_inverse_fp<LOGN, P + 1, REDUCE>(e, tid, T, ssm);
   } else {
 #pragma unroll
     for (int v = 0; v < 8; ++v) e[v] = fp_mulmod(e[v], T.ninv_d[LOGN], T.qd, T.qinv);

@@ -264,7 +264,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_dmux_fp(u64* __restrict_
   const u64 qi = R.m[l].q;
   u64* o0 = out + (2 * o) * 2 * nl * n;
   u64* o1 = o0 + 2 * nl * n;
-  ntt_inverse_fp<LOGN>(am, tid, T, ssm);
+  ntt_inverse_fp<LOGN, 0, true>(am, tid, T, ssm);
 #pragma unroll
   for (int v = 0; v < 8; ++v) {  // ext mask
     const long at = (long)l * n + InL::index(v, tid);
@@ -273,7 +273,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_dmux_fp(u64* __restrict_
     o1[at] = ext;
   }
   __syncthreads();  // the body's transform reuses the exchange area
-  ntt_inverse_fp<LOGN>(ab, tid, T, ssm);
+  ntt_inverse_fp<LOGN, 0, true>(ab, tid, T, ssm);
 #pragma unroll
   for (int v = 0; v < 8; ++v) {  // ext body
     const long at = (long)(nl + l) * n + InL::index(v, tid);
