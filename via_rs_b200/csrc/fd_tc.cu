@@ -6,9 +6,10 @@
 // selection, issues the byte-product MMAs into a TMEM accumulator, and an
 // epilogue folds the accumulator columns into residues mod q2.
 //
-// Warp roles (320 threads): warp 0 lane 0 issues the bulk copies, warp 1
+// Warp roles (352 threads): warp 0 lane 0 issues the bulk copies, warp 1
 // allocates TMEM and its lane 0 issues the MMAs, warps 2..9 read TMEM and write
-// the outputs. Every wait is bounded in time; when one runs out the CTA raises
+// the outputs, and warp 10 expands the two-bit top byte plane of packed chunks
+// (fd_tc.cuh) in shared memory before the MMAs read it. Every wait is bounded in time; when one runs out the CTA raises
 // an error word and leaves its loops instead of waiting on.
 //
 // Accumulator placement. The selection chunk stacks the five byte limbs of the
@@ -26,7 +27,8 @@ namespace via {
 namespace {
 
 constexpr int EPI_WARPS = 8;
-constexpr int FD_THREADS = 64 + 32 * EPI_WARPS;
+constexpr int UNPACK_WARP = 2 + EPI_WARPS;
+constexpr int FD_THREADS = 64 + 32 * EPI_WARPS + 32;
 constexpr int ZERO_TILE = 256 * 32;  // zero operand for clearing grouped accumulators
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 constexpr unsigned WAIT_SPINS = 1u << 26;
@@ -38,6 +40,7 @@ struct KParams {
   int* err;
   int n, J, n_jt, n_kc, n_ct, N, Np, nq;
   int stages, grouped, acc_stride, nacc, tmem_cols, order;
+  int packed4, chunk, stage_bytes, sel_off, unp_off;  // chunk layout (FD_CHUNK or FD_CHUNK_P4) and stage offsets
   unsigned fault_ns;  // test hook: > 0 makes the epilogue's first wait run out after this long
   DevMod m;
 };
@@ -175,11 +178,12 @@ __device__ __forceinline__ u64 fold9(const u32 (&v)[9], const DevMod& m) {
 
 __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
   extern __shared__ __align__(1024) uint8_t smem[];
-  const int stage_bytes = FD_CHUNK + P.Np * FD_KC;
+  const int stage_bytes = P.stage_bytes;
   uint8_t* zero_tile = smem + (size_t)P.stages * stage_bytes;
   u64* full = reinterpret_cast<u64*>(zero_tile + ZERO_TILE);
   u64* empty = full + P.stages;
-  u64* acc_full = empty + P.stages;
+  u64* unp = empty + P.stages;  // packed chunks: the stage's top byte plane is expanded
+  u64* acc_full = unp + P.stages;
   u64* acc_empty = acc_full + 2;
   u64* drain = acc_empty + 2;
   u64* never = drain + 1;  // the test hook's barrier: initialised, never arrived on
@@ -191,6 +195,7 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
     for (int s = 0; s < P.stages; ++s) {
       mbar_init(full + s, 1);
       mbar_init(empty + s, 1);
+      mbar_init(unp + s, 1);
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(acc_full + a, 1);
@@ -229,7 +234,7 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
         int t, ct;
         unit_coords(P, u, t, ct);
         const uint8_t* selu = P.sel + ((size_t)t * P.n_ct + ct) * P.n_kc * sel_chunk;
-        const uint8_t* dbt = P.db + (size_t)t * P.n_jt * P.n_kc * FD_CHUNK;
+        const uint8_t* dbt = P.db + (size_t)t * P.n_jt * P.n_kc * P.chunk;
         for (int jt = 0; ok && jt < P.n_jt; ++jt)
           for (int kc = 0; kc < P.n_kc; ++kc) {
             if (!mbar_wait(empty + s, ph ^ 1, abort_flag)) {
@@ -237,9 +242,9 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
               break;
             }
             uint8_t* dst = smem + (size_t)s * stage_bytes;
-            mbar_expect_tx(full + s, FD_CHUNK + sel_chunk);
-            bulk_g2s(dst, dbt + ((size_t)jt * P.n_kc + kc) * FD_CHUNK, FD_CHUNK, full + s);
-            bulk_g2s(dst + FD_CHUNK, selu + (size_t)kc * sel_chunk, sel_chunk, full + s);
+            mbar_expect_tx(full + s, (u32)P.chunk + sel_chunk);
+            bulk_g2s(dst, dbt + ((size_t)jt * P.n_kc + kc) * P.chunk, (u32)P.chunk, full + s);
+            bulk_g2s(dst + P.sel_off, selu + (size_t)kc * sel_chunk, sel_chunk, full + s);
             armed |= 1u << s;
             armed_par = (armed_par & ~(1u << s)) | (ph << s);
             if (++s == P.stages) {
@@ -278,18 +283,20 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
           if (P.grouped)  // columns [4N, 9N) start at zero; [0, 5N) are set by the first limb-0 product.
             mma_u8(dacc + 4 * P.N, smem_desc(zero_addr, lbo_a, 128), smem_desc(zero_addr, lbo_b, 128), idesc, 0);
           for (int kc = 0; kc < P.n_kc; ++kc) {
-            if (!mbar_wait(full + s, ph, abort_flag)) {
+            // Packed chunks: the stage's copies have landed and its top plane is expanded.
+            if (!mbar_wait(full + s, ph, abort_flag) || (P.packed4 && !mbar_wait(unp + s, ph, abort_flag))) {
               ok = false;
               break;
             }
             tc_fence_after();
             const u32 sa = smem_addr(smem + (size_t)s * stage_bytes);
-            const u32 sb = sa + FD_CHUNK;
+            const u32 sb = sa + (u32)P.sel_off;
+            const u32 a4 = P.packed4 ? sa + (u32)P.unp_off : sa + 4 * FD_PLANE;  // the top byte plane
 #pragma unroll
             for (int ks = 0; ks < FD_KC / 32; ++ks) {
 #pragma unroll
               for (int k = 0; k < FD_LIMBS; ++k) {
-                const u64 ad = smem_desc(sa + k * (FD_MT * FD_KC) + ks * 2 * lbo_a, lbo_a, 128);
+                const u64 ad = smem_desc((k == 4 ? a4 : sa + k * FD_PLANE) + ks * 2 * lbo_a, lbo_a, 128);
                 const u64 bd = smem_desc(sb + ks * 2 * lbo_b, lbo_b, 128);
                 const u32 col = P.grouped ? (u32)(k * P.N) : (u32)(16 * k);
                 const u32 accum = (kc == 0 && ks == 0) ? (P.grouped ? (k > 0) : 0u) : 1u;
@@ -317,6 +324,47 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
       // Every MMA issued above completes before TMEM is released.
       mma_commit(drain);
       if (!mbar_wait(drain, 0, abort_flag, false)) atomicOr(P.err, 2);
+    }
+  } else if (warp == UNPACK_WARP) {
+    // ---- Packed chunks: expand the top byte plane of each landed stage
+    // (fd_tc.cuh layout) into the stage's unpacked area, then release it to
+    // the MMAs. The same walk over units, column tiles and row chunks as the
+    // MMA issuer; a wait that runs out aborts the CTA.
+    if (P.packed4) {
+      int s = 0;
+      u32 ph = 0;
+      bool ok = true;
+      for (int u = blockIdx.x; ok && u < units; u += gridDim.x)
+        for (int jt = 0; ok && jt < P.n_jt; ++jt)
+          for (int kc = 0; kc < P.n_kc; ++kc) {
+            if (!__all_sync(0xffffffffu, mbar_wait(full + s, ph, abort_flag))) {
+              ok = false;
+              break;
+            }
+            uint8_t* stg = smem + (size_t)s * stage_bytes;
+            const uint4* pk = reinterpret_cast<const uint4*>(stg + 4 * FD_PLANE);
+            uint4* up = reinterpret_cast<uint4*>(stg + P.unp_off);
+#pragma unroll
+            for (int i = 0; i < FD_PACK4 / 16 / 32; ++i) {  // four quads per lane
+              const int Q = lane + 32 * i;
+              const uint4 w = pk[Q];
+#pragma unroll
+              for (int k = 0; k < 4; ++k)
+                up[4 * Q + k] = make_uint4((w.x >> (2 * k)) & 0x03030303u, (w.y >> (2 * k)) & 0x03030303u,
+                                           (w.z >> (2 * k)) & 0x03030303u, (w.w >> (2 * k)) & 0x03030303u);
+            }
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");  // visible to the MMAs' async proxy
+            __syncwarp();
+            if (lane == 0) mbar_arrive(unp + s);
+            if (++s == P.stages) {
+              s = 0;
+              ph ^= 1;
+            }
+          }
+      if (!ok && lane == 0) {
+        atomicOr(P.err, 8);
+        *abort_flag = 1;
+      }
     }
   } else {
     // ---- Epilogue: TMEM -> residues mod q2 -> out[b][j][mb][t].
@@ -456,8 +504,10 @@ __global__ void k_fd_split(const u64* __restrict__ sel, int nq, int I, int n, in
 }
 
 // Database rows [i0, i0 + 16) (u64 [16][J][n]) -> byte planes. One thread per (t, j).
+// Packed chunks (packed4): the top byte goes to the two-bit plane, OR-ed into
+// the quad words the four threads of a group quad share (the planes start zeroed).
 __global__ void k_fd_planes(const u64* __restrict__ stage, int i0, int I, int J, int n, int n_jt, int n_kc,
-                            uint8_t* __restrict__ planes) {
+                            int packed4, uint8_t* __restrict__ planes) {
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   if (gid >= (long)J * n) return;
   const int t = (int)(gid % n), j = (int)(gid / n);
@@ -474,19 +524,39 @@ __global__ void k_fd_planes(const u64* __restrict__ stage, int i0, int I, int J,
   }
   const int kc = i0 / FD_KC, kk = (i0 % FD_KC) / 16;
   const int jt = j / FD_MT, r = j % FD_MT;
-  uint8_t* base = planes + (((size_t)t * n_jt + jt) * n_kc + kc) * FD_CHUNK;
+  const int chunk = packed4 ? FD_CHUNK_P4 : FD_CHUNK;
+  uint8_t* base = planes + (((size_t)t * n_jt + jt) * n_kc + kc) * chunk;
+  const int G = (kk * (FD_MT / 8) + r / 8) * 8 + r % 8;  // this thread's 16-byte group in every plane
+  const int planes_full = packed4 ? 4 : FD_LIMBS;
 #pragma unroll
   for (int l = 0; l < FD_LIMBS; ++l)
-    *reinterpret_cast<uint4*>(base + (size_t)l * FD_MT * FD_KC + ((size_t)kk * (FD_MT / 8) + r / 8) * 128 +
-                              (r % 8) * 16) = make_uint4(w[l][0], w[l][1], w[l][2], w[l][3]);
+    if (l < planes_full)
+      *reinterpret_cast<uint4*>(base + (size_t)l * FD_PLANE + (size_t)G * 16) =
+          make_uint4(w[l][0], w[l][1], w[l][2], w[l][3]);
+  if (packed4) {
+    // Byte 4w + b of group 4Q + k -> bits 8b + 2k of word w of quad Q; the top
+    // bytes are below 4.
+    unsigned int* pq = reinterpret_cast<unsigned int*>(base + 4 * FD_PLANE) + (G >> 2) * 4;
+    const int k = G & 3;
+#pragma unroll
+    for (int ww = 0; ww < 4; ++ww) {
+      const u32 bits = (w[4][ww] & 0x03030303u) << (2 * k);
+      if (bits) atomicOr(pq + ww, bits);
+    }
+  }
 }
+
+// Bytes of one shared-memory stage ahead of its selection chunk: the planes,
+// and for packed chunks the expanded top plane after them.
+constexpr int fd_stage_planes(bool packed4) { return packed4 ? FD_CHUNK_P4 + FD_PLANE : FD_CHUNK; }
 
 struct Tiling {
   int grouped, N, Np, n_ct, stages, acc_stride, nacc, tmem_cols, order;
   size_t smem;
 };
 
-Tiling tiling(int nq, const FdTile& tile) {
+// packed4: stages hold FD_CHUNK_P4 bytes of planes, then the expanded top plane.
+Tiling tiling(int nq, const FdTile& tile, bool packed4) {
   Tiling T{};
   int acc_cols;
   if (nq == 1) {
@@ -515,7 +585,7 @@ Tiling tiling(int nq, const FdTile& tile) {
   int cols = T.nacc * T.acc_stride, p2 = 32;
   while (p2 < cols) p2 <<= 1;
   T.tmem_cols = p2;
-  T.smem = (size_t)T.stages * (FD_CHUNK + (size_t)T.Np * FD_KC) + ZERO_TILE + 256;
+  T.smem = (size_t)T.stages * (fd_stage_planes(packed4) + (size_t)T.Np * FD_KC) + ZERO_TILE + 256;
   return T;
 }
 
@@ -524,8 +594,9 @@ constexpr int SMEM_DEFAULT = 200 * 1024;
 
 }  // namespace
 
-size_t fd_planes_bytes(int I, int J, int n) {
-  return (size_t)fd_round_up(I, FD_KC) * fd_round_up(J, FD_MT) * n * FD_LIMBS;
+size_t fd_planes_bytes(int I, int J, int n, bool packed4) {
+  return (size_t)(fd_round_up(I, FD_KC) / FD_KC) * (fd_round_up(J, FD_MT) / FD_MT) * n *
+         (packed4 ? FD_CHUNK_P4 : FD_CHUNK);
 }
 
 bool fd_supported(int I, int n, u64 q) { return I >= 1 && I <= 4096 && n >= 1 && q < (1ull << 40); }
@@ -536,7 +607,7 @@ bool fd_tile_valid(const FdPlan& p, int nq, const FdTile& t) {
   if (t.stages != 0 && (t.stages < 2 || t.stages > 6)) return false;
   if (t.order != 0 && t.order != 1) return false;
   if (nq == 1 && (t.n_max != 0 || t.order != 0)) return false;
-  const Tiling T = tiling(nq, t);
+  const Tiling T = tiling(nq, t, p.packed4);
   const size_t limit = p.smem_max > 0 ? (size_t)p.smem_max : (size_t)SMEM_DEFAULT;
   return T.Np <= 256 && T.nacc * T.acc_stride <= 512 && T.smem <= limit;
 }
@@ -566,10 +637,10 @@ std::vector<FdTile> fd_tile_candidates(const FdPlan& p, int nq) {
   std::vector<FdTile> out;
   out.push_back(FdTile{});  // the default first
   auto add = [&](FdTile t) {
-    const Tiling a = tiling(nq, t);
+    const Tiling a = tiling(nq, t, p.packed4);
     if (!fd_tile_valid(p, nq, t)) return;
     for (const FdTile& o : out) {  // skip tiles that launch the same kernel configuration
-      const Tiling b = tiling(nq, o);
+      const Tiling b = tiling(nq, o, p.packed4);
       if (a.N == b.N && a.n_ct == b.n_ct && a.stages == b.stages && a.order == b.order) return;
     }
     out.push_back(t);
@@ -587,7 +658,7 @@ std::vector<FdTile> fd_tile_candidates(const FdPlan& p, int nq) {
 void fd_rows_to_planes(const u64* stage, int i0, const FdPlan& p, uint8_t* planes, cudaStream_t st) {
   const long total = (long)p.J * p.n;
   k_fd_planes<<<(unsigned)((total + 255) / 256), 256, 0, st>>>(stage, i0, p.I, p.J, p.n, p.J_pad / FD_MT,
-                                                              p.I_pad / FD_KC, planes);
+                                                              p.I_pad / FD_KC, p.packed4 ? 1 : 0, planes);
   VIA_LAUNCHED();
 }
 
@@ -595,7 +666,7 @@ size_t fd_sel_bytes(const FdPlan& p, int nq) {
   // Every candidate's split selection: n * n_ct * Np * I_pad bytes.
   size_t bytes = 0;
   for (const FdTile& t : fd_tile_candidates(p, nq)) {
-    const Tiling T = tiling(nq, t);
+    const Tiling T = tiling(nq, t, p.packed4);
     bytes = std::max(bytes, (size_t)p.n * T.n_ct * (size_t)T.Np * p.I_pad);
   }
   return bytes;
@@ -614,7 +685,7 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
              const FdTile* force) {
   const FdTile tile = force ? *force : fd_tile_for(p, nq);
   if (force && !fd_tile_valid(p, nq, tile)) throw CudaError(100, "scan tile not valid for this batch");
-  const Tiling T = tiling(nq, tile);
+  const Tiling T = tiling(nq, tile, p.packed4);
   const int n_k16 = p.I_pad / 16, n_kc = p.I_pad / FD_KC;
   const int pad = T.grouped ? T.Np - FD_LIMBS * T.N : 0;
   const long total = (long)p.n * T.n_ct * (T.N + pad) * n_k16;
@@ -640,6 +711,11 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
   K.nacc = T.nacc;
   K.tmem_cols = T.tmem_cols;
   K.order = T.order;
+  K.packed4 = p.packed4 ? 1 : 0;
+  K.chunk = p.packed4 ? FD_CHUNK_P4 : FD_CHUNK;
+  K.stage_bytes = fd_stage_planes(p.packed4) + T.Np * FD_KC;
+  K.sel_off = fd_stage_planes(p.packed4);
+  K.unp_off = FD_CHUNK_P4;
   K.fault_ns = p.fault_wait_ns;
   K.m = p.m;
   const int units = p.n * T.n_ct;

@@ -20,13 +20,22 @@ namespace via {
 
 // Byte-plane layout of the prepared database (built once at setup):
 //   [t][jt][kc][limb][128 x 64 bytes in the tensor-core K-major core-matrix order]
-// jt = j / 128, kc = i / 64; every (t, jt, kc) chunk of 5 * 128 * 64 bytes is
-// contiguous, so one bulk copy moves it into shared memory. Rows i >= I and
-// columns j >= J are zero.
+// jt = j / 128, kc = i / 64; every (t, jt, kc) chunk (5 * 128 * 64 bytes, or
+// the packed layout below) is contiguous, so one bulk copy moves it into shared
+// memory. Rows i >= I and columns j >= J are zero.
 constexpr int FD_KC = 64;     // bytes of the reduction (row) dimension per chunk
 constexpr int FD_MT = 128;    // database columns per MMA tile (the M dimension)
 constexpr int FD_LIMBS = 5;   // bytes per residue
-constexpr int FD_CHUNK = FD_LIMBS * FD_MT * FD_KC;  // 40960 bytes
+constexpr int FD_PLANE = FD_MT * FD_KC;             // 8192 bytes: one byte plane of a chunk
+constexpr int FD_CHUNK = FD_LIMBS * FD_PLANE;       // 40960 bytes
+// Packed chunks (q2 < 2^34, so byte 4 of a residue is below 4): planes 0..3 as
+// above, then byte 4 at two bits per residue (2048 bytes): for every quad Q of
+// four consecutive 16-byte groups of the unpacked plane (groups 4Q .. 4Q + 3 in
+// core-matrix order), four u32 words P_w, w < 4, where bits 8b + 2k, 8b + 2k + 1
+// of P_w hold byte 4w + b of group 4Q + k. Unpacking a group is then one shift
+// and one mask per word: word w of group 4Q + k = (P_w >> 2k) & 0x03030303.
+constexpr int FD_PACK4 = FD_PLANE / 4;                 // 2048 bytes
+constexpr int FD_CHUNK_P4 = 4 * FD_PLANE + FD_PACK4;   // 34816 bytes
 
 // One scan tile choice, the autotuner's search space. Every choice computes the
 // same exact sums; they differ in speed only.
@@ -52,6 +61,7 @@ struct FdPlan {
   DevMod m{};
   int grid = 148;          // persistent CTAs (one per SM)
   int smem_max = 0;        // opt-in shared memory per block on this device
+  bool packed4 = false;    // chunks in the packed layout (FD_CHUNK_P4 bytes each)
   int* err = nullptr;      // device word: nonzero after a bounded wait ran out
   // Test hook (via_server_set_scan_fault): when nonzero, the epilogue of every
   // CTA first waits on a barrier that nothing completes, bounded by this many
@@ -64,7 +74,9 @@ struct FdPlan {
 };
 
 inline int fd_round_up(int v, int a) { return (v + a - 1) / a * a; }
-size_t fd_planes_bytes(int I, int J, int n);
+size_t fd_planes_bytes(int I, int J, int n, bool packed4);
+// The packed layout serves moduli below 2^34.
+inline bool fd_packable(u64 q) { return q < (1ull << 34); }
 bool fd_supported(int I, int n, u64 q);
 
 // The tile a scan of nq queries runs with (tuned entry or default).

@@ -260,10 +260,11 @@ static void setup(Server& s, const via_params& p, const via_public_keys* keys, c
     s.fd.I_pad = fd_round_up((int)I, FD_KC);
     s.fd.J_pad = fd_round_up((int)J, FD_MT);
     s.fd.m = s.r2.m[0];
+    s.fd.packed4 = fd_packable(p.q2);
     VIA_CUDA(cudaDeviceGetAttribute(&s.fd.grid, cudaDevAttrMultiProcessorCount, s.device));
     s.fd.smem_max = fd_prepare_device();
     s.planes = std::make_shared<DevBuf>();
-    s.planes->alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1) / 8);
+    s.planes->alloc(fd_planes_bytes((int)I, (int)J, (int)p.n1, s.fd.packed4) / 8);
     VIA_CUDA(cudaMemsetAsync(s.planes->p, 0, s.planes->n * 8, s.stream));
     s.fd_err.alloc(1);
     VIA_CUDA(cudaMemsetAsync(s.fd_err.p, 0, 8, s.stream));
@@ -546,7 +547,7 @@ std::string tune_key(const Server& s, int nq) {
   std::string dev = prop.name;
   for (char& c : dev)
     if (c == ' ' || c == '\t') c = '_';
-  return "fd_tc/1 " + dev + " n=" + std::to_string(s.fd.n) + " I=" + std::to_string(s.fd.I) +
+  return "fd_tc/2 " + dev + " n=" + std::to_string(s.fd.n) + " I=" + std::to_string(s.fd.I) +
          " J=" + std::to_string(s.fd.J) + " q=" + std::to_string(s.fd.m.q) + " nq=" + std::to_string(nq);
 }
 
