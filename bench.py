@@ -41,12 +41,12 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "answers/s and DB GB/s scanned, batched vs plain, 1 GiB DB; p50/p99 answer ms"
 # ncu dram__bytes_read.sum + dram__bytes_write.sum of one k_fd_tc launch on the
-# I=64, J=4096 paper case: 2.749080 GB read, 174.374656 MB written. Reads scale
-# with the database cells (each cell's 5 * n1 plane bytes are read once, plus the
-# selection chunks that miss L2), writes with the columns (2 * n1 u64 residues
-# per column, written as partial sectors).
-SCAN_READ_BYTES_PER_CELL = 2.749080e9 / (64 * 4096)
-SCAN_WRITE_BYTES_PER_COLUMN = 174.374656e6 / 4096
+# I=64, J=4096 paper case (packed planes, q2 < 2^34): 2.284716288 GB read,
+# 130.85696 MB written. Reads scale with the database cells (each cell's
+# 4.25 * n1 plane bytes are read once, plus the selection chunks that miss L2),
+# writes with the columns (2 * n1 u64 residues per column).
+SCAN_READ_BYTES_PER_CELL = 2.284716288e9 / (64 * 4096)
+SCAN_WRITE_BYTES_PER_COLUMN = 130.85696e6 / 4096
 
 
 def prepared_db_bytes(prm):

@@ -1385,7 +1385,7 @@ static void resp_comp(Server& s, Workspace& w, const u64* ct_q2, long B, u64* d_
 void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u64* d_mask, u64* d_body,
                           cudaStream_t st, int stop_stage, u64* dump) {
   const via_params& p = s.prm;
-  const int n1 = p.n1, n2 = p.n2, L = p.l_query, nl = s.r1.nl;
+  const int n1 = p.n1, L = p.l_query, nl = s.r1.nl;
   const long I = p.num_rows, J = p.num_cols, B = nq;
   const int nd = ilog2(I), nc = ilog2(J);
   const int nr = (int)(w.nbits - nd - nc);
