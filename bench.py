@@ -80,6 +80,8 @@ def parse():
     ap.add_argument("--no-autotune", action="store_true", help="keep the default scan tiles (skip the autotuner)")
     ap.add_argument("--microbench", type=int, default=1, help="run the kernel micro-benchmark leg (NTT, external "
                     "product, key switch at n = 2048)")
+    ap.add_argument("--scan-tile", default="",
+                    help="n_max,stages,order: force this scan tile for --batch queries (after any autotuning)")
     ap.add_argument("--profile-batch", action="store_true",
                     help="set up, answer one batch of --batch queries and exit (a short target for ncu)")
     return ap.parse_args()
@@ -693,6 +695,9 @@ def gpu_arm(args, prm):
     tuning = []
     if not args.no_autotune:
         tuning = server.autotune([1] + ([args.batch] if args.batch > 1 else []))
+    if args.scan_tile:
+        nm, st, od = (int(v) for v in args.scan_tile.split(","))
+        server.set_scan_tile(max(1, args.batch), {"n_max": nm, "stages": st, "order": od})
 
     if args.profile_batch:
         B = max(1, args.batch)

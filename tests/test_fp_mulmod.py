@@ -1,4 +1,5 @@
-"""The double-precision modular product of via_rs_b200/csrc/ntt_fp.cuh, checked on the host.
+"""The double-precision modular product of via_rs_b200/csrc/ntt_fp.cuh, checked on the host,
+and the scan epilogue's fold of nine accumulator groups built on it (fd_tc.cu fold9).
 
 fp_mulmod(a, b) computes, with IEEE-754 double operations rounded to nearest:
     ph = a * b;  pl = fma(a, b, -ph);  qt = (fma(ph, qinv, R) - R);  r = fma(-qt, q, ph) + pl
@@ -64,3 +65,28 @@ def test_canonical_reduction(q):
     for x in list(rng.integers(-(1 << 50) + 1, 1 << 50, size=2000)) + [0, q, -q, q - 1, 1 - q, 8 * q, -8 * q]:
         r = fp_canonical(float(int(x)), qd, qinv)
         assert 0 <= r < q and (int(x) - int(r)) % q == 0
+
+
+def fold9(v, q):
+    """fd_tc.cu fold9: sum_g v_g 2^(8g) mod q from the groups 0-2, 3-5, 6-8."""
+    qd, qinv = float(q), 1.0 / float(q)
+    lo = v[0] + (v[1] << 8) + (v[2] << 16)
+    m1 = v[3] + (v[4] << 8) + (v[5] << 16)
+    m2 = v[6] + (v[7] << 8) + (v[8] << 16)
+    assert max(lo, m1, m2) < 1 << 48
+    r1 = fp_mulmod(float(m1), float((1 << 24) % q), qd, qinv)
+    r2 = fp_mulmod(float(m2), float((1 << 48) % q), qd, qinv)
+    return fp_canonical((float(lo) + r1) + r2, qd, qinv)
+
+
+@pytest.mark.parametrize("q", [m for m in MODULI if m < 1 << 40] + [1_099_511_480_321])
+def test_fold9_exact(q):
+    """Group sums below 2^31 (the TMEM accumulators of a scan over at most 4096 rows)."""
+    rng = np.random.default_rng(q % 4093)
+    top = (1 << 31) - 1
+    cases = [[int(x) for x in row] for row in rng.integers(0, 1 << 31, size=(3000, 9))]
+    cases += [[top] * 9, [0] * 9, [1] * 9, [top if g % 2 else 0 for g in range(9)], [0] * 8 + [top]]
+    for v in cases:
+        want = sum(x << (8 * g) for g, x in enumerate(v)) % q
+        got = fold9(v, q)
+        assert got == want, (q, v, got, want)

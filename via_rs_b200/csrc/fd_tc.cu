@@ -6,11 +6,13 @@
 // selection, issues the byte-product MMAs into a TMEM accumulator, and an
 // epilogue folds the accumulator columns into residues mod q2.
 //
-// Warp roles (352 threads): warp 0 lane 0 issues the bulk copies, warp 1
-// allocates TMEM and its lane 0 issues the MMAs, warps 2..9 read TMEM and write
-// the outputs, and warp 10 expands the two-bit top byte plane of packed chunks
-// (fd_tc.cuh) in shared memory before the MMAs read it. Every wait is bounded in time; when one runs out the CTA raises
-// an error word and leaves its loops instead of waiting on.
+// Warp roles (64 + 32 EPI + 32 threads): warp 0 lane 0 issues the bulk copies,
+// warp 1 allocates TMEM and its lane 0 issues the MMAs, the EPI warps 2 ..
+// EPI + 1 read TMEM and write the outputs (8 for one query, 16 for grouped
+// tiles), and the last warp expands the two-bit top byte plane of packed
+// chunks (fd_tc.cuh) in shared memory before the MMAs read it. Every wait is
+// bounded in time; when one runs out the CTA raises an error word and leaves
+// its loops instead of waiting on.
 //
 // Accumulator placement. The selection chunk stacks the five byte limbs of the
 // N columns of a c-tile as rows l*N + c of the MMA's N dimension. The MMA of
@@ -22,13 +24,15 @@
 #include <algorithm>
 
 #include "fd_tc.cuh"
+#include "ntt_fp.cuh"
 
 namespace via {
 namespace {
 
-constexpr int EPI_WARPS = 8;
-constexpr int UNPACK_WARP = 2 + EPI_WARPS;
-constexpr int FD_THREADS = 64 + 32 * EPI_WARPS + 32;
+// Epilogue warps: 8 for the single-query tile, 16 for grouped tiles, whose
+// epilogue (nine TMEM groups folded per output) sets the pace of a batch.
+constexpr int EPI_ONE = 8, EPI_GROUPED = 16;
+constexpr int fd_threads(int epi) { return 64 + 32 * epi + 32; }
 constexpr int ZERO_TILE = 256 * 32;  // zero operand for clearing grouped accumulators
 constexpr unsigned long long WAIT_NS = 2000000000ull;  // 2 s per wait
 constexpr unsigned WAIT_SPINS = 1u << 26;
@@ -42,7 +46,7 @@ struct KParams {
   int stages, grouped, acc_stride, nacc, tmem_cols, order;
   int packed4, chunk, stage_bytes, sel_off, unp_off;  // chunk layout (FD_CHUNK or FD_CHUNK_P4) and stage offsets
   unsigned fault_ns;  // test hook: > 0 makes the epilogue's first wait run out after this long
-  DevMod m;
+  double qd, qinv, c24, c48;  // q2, its rounded inverse, 2^24 and 2^48 mod q2, as doubles
 };
 
 __device__ __forceinline__ u32 smem_addr(const void* p) { return (u32)__cvta_generic_to_shared(p); }
@@ -133,6 +137,11 @@ __device__ __forceinline__ void mma_commit(u64* bar) {
                : "memory");
 }
 
+__device__ __forceinline__ void tmem_ld4(u32 taddr, u32 (&r)[4]) {
+  asm volatile("tcgen05.ld.sync.aligned.32x32b.x4.b32 {%0, %1, %2, %3}, [%4];"
+               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+               : "r"(taddr));
+}
 __device__ __forceinline__ void tmem_ld8(u32 taddr, u32 (&r)[8]) {
   asm volatile("tcgen05.ld.sync.aligned.32x32b.x8.b32 {%0, %1, %2, %3, %4, %5, %6, %7}, [%8];"
                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7])
@@ -147,6 +156,13 @@ __device__ __forceinline__ void tmem_ld16(u32 taddr, u32 (&r)[16]) {
       : "r"(taddr));
 }
 __device__ __forceinline__ void tmem_wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
+template <int W>
+__device__ __forceinline__ void tmem_ld(u32 taddr, u32 (&r)[W]) {
+  if constexpr (W == 4)
+    tmem_ld4(taddr, r);
+  else
+    tmem_ld8(taddr, r);
+}
 // Orders later uses of r after the wait above (the loads' results are only
 // defined once tcgen05.wait::ld has returned).
 template <int K>
@@ -166,17 +182,34 @@ __device__ __forceinline__ void unit_coords(const KParams& P, int u, int& t, int
   }
 }
 
-// sum_g v_g 2^{8g} mod q for nine group sums v_g < 2^31.
-__device__ __forceinline__ u64 fold9(const u32 (&v)[9], const DevMod& m) {
-  const u64 lo = (u64)v[0] + ((u64)v[1] << 8) + ((u64)v[2] << 16) + ((u64)v[3] << 24);
-  const u64 hi = (u64)v[4] + ((u64)v[5] << 8) + ((u64)v[6] << 16) + ((u64)v[7] << 24) + ((u64)v[8] << 32);
-  // lo + hi * 2^32 as 128 bits.
-  const u64 s_lo = lo + (hi << 32);
-  const u64 s_hi = (hi >> 32) + (s_lo < lo ? 1 : 0);
-  return reduce128(s_hi, s_lo, m);
+// Integers below 2^52 to and from doubles, exactly: the double 2^52 + x has the
+// bit pattern 0x4330000000000000 | x.
+__device__ __forceinline__ double u52_to_double(u64 x) {
+  return __dadd_rn(__longlong_as_double((long long)(x | 0x4330000000000000ull)), -4503599627370496.0);
+}
+__device__ __forceinline__ u64 double_to_u52(double x) {
+  return (u64)__double_as_longlong(__dadd_rn(x, 4503599627370496.0)) & 0xFFFFFFFFFFFFFull;
 }
 
-__global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
+// sum_g v_g 2^{8g} mod q for nine group sums v_g < 2^31 and q < 2^40, on the
+// FP64 pipe: with lo, m1, m2 the sums of groups 0-2, 3-5 and 6-8 at their own
+// scale (each below 2^31 (1 + 2^8 + 2^16) < 2^48), the value is
+// lo + m1 2^24 + m2 2^48, and lo + fp_mulmod(m1, 2^24 mod q) + fp_mulmod(m2,
+// 2^48 mod q) is an integer of magnitude below 2^48 + 1.125 q (ntt_fp.cuh
+// bounds), which fp_canonical brings into [0, q).
+__device__ __forceinline__ u64 fold9(const u32 (&v)[9], const KParams& P) {
+  const u64 lo = (u64)v[0] + ((u64)v[1] << 8) + ((u64)v[2] << 16);
+  const u64 m1 = (u64)v[3] + ((u64)v[4] << 8) + ((u64)v[5] << 16);
+  const u64 m2 = (u64)v[6] + ((u64)v[7] << 8) + ((u64)v[8] << 16);
+  const double r1 = fp_mulmod(u52_to_double(m1), P.c24, P.qd, P.qinv);
+  const double r2 = fp_mulmod(u52_to_double(m2), P.c48, P.qd, P.qinv);
+  const double s = __dadd_rn(__dadd_rn(u52_to_double(lo), r1), r2);
+  return double_to_u52(fp_canonical(s, P.qd, P.qinv));
+}
+
+template <int EPI>
+__global__ void __launch_bounds__(fd_threads(EPI), 1) k_fd_tc(KParams P) {
+  constexpr int UNPACK_WARP = 2 + EPI;
   extern __shared__ __align__(1024) uint8_t smem[];
   const int stage_bytes = P.stage_bytes;
   uint8_t* zero_tile = smem + (size_t)P.stages * stage_bytes;
@@ -199,7 +232,7 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
     }
     for (int a = 0; a < 2; ++a) {
       mbar_init(acc_full + a, 1);
-      mbar_init(acc_empty + a, EPI_WARPS * 32);
+      mbar_init(acc_empty + a, EPI * 32);
     }
     mbar_init(drain, 1);
     mbar_init(never, 1);
@@ -367,8 +400,10 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
       }
     }
   } else {
-    // ---- Epilogue: TMEM -> residues mod q2 -> out[b][j][mb][t].
-    const int ew = warp - 2, quad = warp & 3, half = ew >> 2;
+    // ---- Epilogue: TMEM -> residues mod q2 -> out[b][j][mb][t]. Warp w
+    // reads TMEM lanes 32 (w % 4) .. + 31 (its lane quadrant: database rows of
+    // the tile); the EPI / 4 warps of a quadrant split the columns.
+    const int ew = warp - 2, quad = warp & 3, part = ew >> 2;
     const int row = quad * 32 + lane;
     int a = 0;
     u32 aph = 0;
@@ -387,36 +422,46 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
         const u32 tb = tmem + (u32)(a * P.acc_stride) + ((u32)(quad * 32) << 16);
         const int j = jt * FD_MT + row;
         const bool jok = j < P.J;
+        bool released = false;
         if (P.grouped) {
-          // 8-column chunks of the tile, alternating between the two halves
-          // (N is a multiple of 8).
-          for (int c0 = half * 8; c0 < P.N; c0 += 16) {
-            u32 v[9][8];
+          // CW-column chunks of the tile, dealt round-robin to the quadrant's
+          // warps (N is a multiple of 8). A warp frees the accumulator once its
+          // last chunk is in registers, so the next tile's MMAs overlap the
+          // folding and stores of that chunk.
+          constexpr int CW = EPI >= 16 ? 4 : 8, STEP = (EPI / 4) * CW;
+          const size_t qs = (size_t)2 * P.J * P.n;  // between queries
+          u64* orow = P.out + (size_t)j * 2 * P.n + t;
+          for (int c0 = part * CW; c0 < P.N; c0 += STEP) {
+            u32 v[9][CW];
 #pragma unroll
-            for (int g = 0; g < 9; ++g) tmem_ld8(tb + (u32)(g * P.N + c0), v[g]);
+            for (int g = 0; g < 9; ++g) tmem_ld<CW>(tb + (u32)(g * P.N + c0), v[g]);
             tmem_wait_ld();
 #pragma unroll
             for (int g = 0; g < 9; ++g) pin(v[g]);
+            if (c0 + STEP >= P.N) {
+              tc_fence_before();
+              mbar_arrive(acc_empty + a);
+              released = true;
+            }
 #pragma unroll
-            for (int x = 0; x < 8; ++x) {
+            for (int x = 0; x < CW; ++x) {
               const int cg = ct * P.N + c0 + x;
               if (jok && cg < 2 * P.nq) {
                 u32 w[9];
 #pragma unroll
                 for (int g = 0; g < 9; ++g) w[g] = v[g][x];
-                const int b = cg >> 1, mb = cg & 1;
-                P.out[(((size_t)b * P.J + j) * 2 + mb) * P.n + t] = fold9(w, P.m);
+                orow[(size_t)(cg >> 1) * qs + (size_t)(cg & 1) * P.n] = fold9(w, P);
               }
             }
           }
-        } else {
+        } else if (part < 2) {
           u32 r[FD_LIMBS][16];
 #pragma unroll
           for (int k = 0; k < FD_LIMBS; ++k) tmem_ld16(tb + (u32)(16 * k), r[k]);
           tmem_wait_ld();
 #pragma unroll
           for (int k = 0; k < FD_LIMBS; ++k) pin(r[k]);
-          // N = 2: half 0 writes the mask column, half 1 the body.
+          // N = 2: part 0 writes the mask column, part 1 the body.
           u32 w0[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0}, w1[9] = {0, 0, 0, 0, 0, 0, 0, 0, 0};
 #pragma unroll
           for (int k = 0; k < FD_LIMBS; ++k)
@@ -427,11 +472,13 @@ __global__ void __launch_bounds__(FD_THREADS, 1) k_fd_tc(KParams P) {
             }
           u32 w[9];
 #pragma unroll
-          for (int g = 0; g < 9; ++g) w[g] = half ? w1[g] : w0[g];
-          if (jok) P.out[((size_t)j * 2 + half) * P.n + t] = fold9(w, P.m);
+          for (int g = 0; g < 9; ++g) w[g] = part ? w1[g] : w0[g];
+          if (jok) P.out[((size_t)j * 2 + part) * P.n + t] = fold9(w, P);
         }
-        tc_fence_before();
-        mbar_arrive(acc_empty + a);
+        if (!released) {
+          tc_fence_before();
+          mbar_arrive(acc_empty + a);
+        }
         if (++a == P.nacc) {
           a = 0;
           aph ^= 1;
@@ -677,7 +724,8 @@ int fd_prepare_device() {
   VIA_CUDA(cudaGetDevice(&dev));
   VIA_CUDA(cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
   const int limit = std::max(optin, SMEM_DEFAULT);
-  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc<EPI_ONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
+  VIA_CUDA(cudaFuncSetAttribute(k_fd_tc<EPI_GROUPED>, cudaFuncAttributeMaxDynamicSharedMemorySize, limit));
   return limit;
 }
 
@@ -717,10 +765,16 @@ void fd_scan(const FdPlan& p, const u64* sel_eval, u64* out_eval, int nq, uint8_
   K.sel_off = fd_stage_planes(p.packed4);
   K.unp_off = FD_CHUNK_P4;
   K.fault_ns = p.fault_wait_ns;
-  K.m = p.m;
+  K.qd = (double)p.m.q;
+  K.qinv = 1.0 / K.qd;
+  K.c24 = (double)(((u64)1 << 24) % p.m.q);
+  K.c48 = (double)(((u64)1 << 48) % p.m.q);
   const int units = p.n * T.n_ct;
   const int grid = std::min(units, p.grid);
-  k_fd_tc<<<grid, FD_THREADS, T.smem, st>>>(K);
+  if (T.grouped)
+    k_fd_tc<EPI_GROUPED><<<grid, fd_threads(EPI_GROUPED), T.smem, st>>>(K);
+  else
+    k_fd_tc<EPI_ONE><<<grid, fd_threads(EPI_ONE), T.smem, st>>>(K);
   VIA_LAUNCHED();
 }
 
