@@ -373,15 +373,18 @@ __global__ void k_cascade_reduce(const u64* __restrict__ P, int rank_in, int N, 
 //   mask_out[j] = -(sum_s D[j][s] K_j[s].mask + D[j+R/2][s] K_{j+R/2}[s].mask)
 //   bsum        =   sum_idx sum_s D[idx][s] K_idx[s].body
 // D: [lwe][idx][L][nl][n_in]; keys: [idx][L][2][nl][n_out]; mask_out:
-// [lwe][R/2][nl][n_out]; bsum: [lwe][nl][n_out]. Block = TT slots x JJ output
-// masks (TT * JJ = 256); the JJ lanes' body partials are summed in shared memory.
-// Small batches give few blocks: the output masks j are then also split over
-// JB blocks (blockIdx.x = slot block * JB + jb), and each block writes its body
-// partial to bpart[lwe][jb][nl][n_out] for k_cascade_bsum to add up.
+// [lwe][R/2][nl][n_out]. Block = TT slots x JJ output masks (TT * JJ = 256); the
+// JJ lanes' body partials are summed in shared memory. The body stays in the
+// eval domain through the cascade: body_out[lwe][l][t] = body_in[lwe][l][t/2] -
+// bsum (the eval form of embed_at(body_in, 0) - bsum, [lwe][nl][n_in] ->
+// [lwe][nl][n_out]). Small batches give few blocks: the output masks j are then
+// also split over JB blocks (blockIdx.x = slot block * JB + jb), and each block
+// writes its body partial to bpart[lwe][jb][nl][n_out] for k_cascade_bsum to add
+// up and apply.
 __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, const u64* __restrict__ keys, int R,
                                                      int n_in, int L, int TT, int JB, DevRing Rg,
-                                                     u64* __restrict__ mask_out, u64* __restrict__ bsum,
-                                                     u64* __restrict__ bpart) {
+                                                     u64* __restrict__ mask_out, const u64* __restrict__ body_in,
+                                                     u64* __restrict__ body_out, u64* __restrict__ bpart) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
@@ -417,7 +420,7 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
     u64 acc = part[tl];
     for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
     if (JB == 1)
-      bsum[(lwe * nl + l) * n_out + t] = acc;
+      body_out[(lwe * nl + l) * n_out + t] = submod(body_in[(lwe * nl + l) * n_in + (t >> 1)], acc, m.q);
     else
       bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
   }
@@ -431,8 +434,8 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
 // Two CTAs per SM leave room for nine digits' loads in flight per thread.
 __global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
                                                         int R, int n_in, int L, int TT, int JB, DevRing Rg,
-                                                        u64* __restrict__ mask_out, u64* __restrict__ bsum,
-                                                        u64* __restrict__ bpart) {
+                                                        u64* __restrict__ mask_out, const u64* __restrict__ body_in,
+                                                        u64* __restrict__ body_out, u64* __restrict__ bpart) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
@@ -469,23 +472,25 @@ __global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restr
     u64 acc = part[tl];
     for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
     if (JB == 1)
-      bsum[(lwe * nl + l) * n_out + t] = acc;
+      body_out[(lwe * nl + l) * n_out + t] = submod(body_in[(lwe * nl + l) * n_in + (t >> 1)], acc, m.q);
     else
       bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
   }
 }
 
-// bsum[lwe][l][t] = sum over jb of bpart[lwe][jb][l][t] (mod q_l).
+// body_out[lwe][l][t] = body_in[lwe][l][t/2] - sum over jb of
+// bpart[lwe][jb][l][t] (mod q_l), all in the eval domain (k_cascade_mac).
 __global__ void k_cascade_bsum(const u64* __restrict__ bpart, int JB, int nl, int n_out, long nlwe, DevRing Rg,
-                               u64* __restrict__ bsum) {
+                               const u64* __restrict__ body_in, u64* __restrict__ body_out) {
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
   const long per = (long)nl * n_out;
   if (gid >= nlwe * per) return;
   const long lwe = gid / per, rem = gid % per;
-  const u64 q = Rg.m[rem / n_out].q;
+  const int l = (int)(rem / n_out), t = (int)(rem % n_out);
+  const u64 q = Rg.m[l].q;
   u64 acc = 0;
   for (int jb = 0; jb < JB; ++jb) acc = addmod(acc, bpart[(lwe * JB + jb) * per + rem], q);
-  bsum[gid] = acc;
+  body_out[gid] = submod(body_in[(lwe * nl + l) * (n_out / 2) + (t >> 1)], acc, q);
 }
 
 // body_out[lwe] = embed_at(body_in[lwe], N_out, 0) - bsum[lwe] (coefficient form).
@@ -858,29 +863,31 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
       if (fp_mac)
         k_cascade_mac_fp<<<grid, 256, 0, st>>>(reinterpret_cast<const double*>(digits),
                                                reinterpret_cast<const double*>(s.cascade_eval_d.p) + k * step_len,
-                                               rank_in, n_in, L, tt, JB, R, mo, bsum, bpart);
+                                               rank_in, n_in, L, tt, JB, R, mo, bi, bo, bpart);
       else
         k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
-                                            bsum, bpart);
+                                            bi, bo, bpart);
       VIA_LAUNCHED();
       if (JB > 1) {
-        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bpart, JB, nl, n_out, nlwe, R, bsum);
+        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bpart, JB, nl, n_out, nlwe, R, bi, bo);
         VIA_LAUNCHED();
       }
+      // The masks return to coefficient form for the next step's digits; the
+      // body stays in the eval domain until the last step.
+      from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
     } else {
       gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), cP,
                      digits, st);
       const long items = nlwe * (rank_in / 2 + 1) * nl * n_out;
       k_cascade_reduce<<<blocks(items), 256, 0, st>>>(cP, rank_in, n_out, nl, nlwe, R, mo, bsum);
       VIA_LAUNCHED();
+      k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, bsum, n_in, nl, nlwe, R, bo);
+      VIA_LAUNCHED();
     }
-    from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
-    from_eval(R, bsum, n_out, nlwe * nl, st);
-    k_cascade_body<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bi, bsum, n_in, nl, nlwe, R, bo);
-    VIA_LAUNCHED();
     std::swap(mi, mo);
     std::swap(bi, bo);
   }
+  if (R.ntt) from_eval(R, bi, n1, nlwe * nl, st);  // the cascade's body, degree n1
   k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, rlwe);
   VIA_LAUNCHED();
   // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178); the
