@@ -283,6 +283,75 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, 2) k_dmux_fp(u64* __restrict_
   }
 }
 
+// Inverse transforms of RLWEs ext ([count][2][nl][n], eval form, canonical) in
+// double precision (ntt_fp.cuh), one CTA per polynomial, with the consumer's
+// elementwise step folded into the stores (coefficient form, canonical):
+//   INTT_STORE: out[j] = ext[j]
+//   INTT_DMUX:  out[2j] = base[j] - ext[j], out[2j+1] = ext[j]  (a DMux level)
+//   INTT_ADD:   out[j] = base[j] + ext[j]                       (a CRot step)
+enum { INTT_STORE = 0, INTT_DMUX = 1, INTT_ADD = 2 };
+template <int LOGN, int MODE>
+__global__ void __launch_bounds__((1 << LOGN) / 8) k_intt_fp_epi(const u64* __restrict__ ext, const u64* base,
+                                                                 u64* out, DevRing R) {
+  constexpr int n = 1 << LOGN;
+  using In0 = NttPhase<LOGN, true, 0>;
+  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
+  static_assert(In0::STRIDE == 1 && In0::R == 3, "contiguous first inverse layout");
+  __shared__ double ssm[n];
+  const int tid = threadIdx.x;
+  const int nl = R.nl;
+  const long seg = blockIdx.x;  // ((j * 2) + part) * nl + limb
+  const int l = (int)(seg % nl);
+  const NttTable& T = R.t[l];
+  const double q = T.qd, qinv = T.qinv;
+  double e[8];
+  const ulonglong2* src = reinterpret_cast<const ulonglong2*>(ext + seg * n + 8 * tid);
+#pragma unroll
+  for (int c = 0; c < 4; ++c) {
+    const ulonglong2 x = src[c];
+    e[2 * c] = __ull2double_rn(x.x);
+    e[2 * c + 1] = __ull2double_rn(x.y);
+  }
+  ntt_inverse_fp<LOGN, 0, true>(e, tid, T, ssm);
+  const u64 qi = R.m[l].q;
+  const long per = 2L * nl * n, j = seg / (2 * nl), at0 = (seg % (2 * nl)) * n;
+#pragma unroll
+  for (int v = 0; v < 8; ++v) {
+    const int x = InL::index(v, tid);
+    const u64 val = __double2ull_rn(fp_canonical(e[v], q, qinv));
+    if constexpr (MODE == INTT_STORE) {
+      out[seg * n + x] = val;
+    } else if constexpr (MODE == INTT_DMUX) {
+      out[(2 * j) * per + at0 + x] = submod(base[j * per + at0 + x], val, qi);
+      out[(2 * j + 1) * per + at0 + x] = val;
+    } else {
+      out[seg * n + x] = addmod(base[seg * n + x], val, qi);
+    }
+  }
+}
+
+// Runs k_intt_fp_epi for `count` RLWEs; false (nothing launched) when the ring
+// has no double-precision transform of this degree.
+template <int MODE>
+static bool intt_epi(const DevRing& R, const u64* ext, const u64* base, u64* out, long count, cudaStream_t st) {
+  if (!R.ntt || !ntt_fp_ok(R.t[0], R.t[R.nl - 1])) return false;
+  const unsigned grid = (unsigned)(count * 2 * R.nl);
+  switch (R.n) {
+    case 4096: k_intt_fp_epi<12, MODE><<<grid, 512, 0, st>>>(ext, base, out, R); break;
+    case 2048: k_intt_fp_epi<11, MODE><<<grid, 256, 0, st>>>(ext, base, out, R); break;
+    case 1024: k_intt_fp_epi<10, MODE><<<grid, 128, 0, st>>>(ext, base, out, R); break;
+    case 512: k_intt_fp_epi<9, MODE><<<grid, 64, 0, st>>>(ext, base, out, R); break;
+    default: return false;
+  }
+  VIA_LAUNCHED();
+  return true;
+}
+
+// Rings whose inverse transforms k_intt_fp_epi serves.
+static bool R_fp_small(const DevRing& R) {
+  return R.ntt && ntt_fp_ok(R.t[0], R.t[R.nl - 1]) && (R.n == 512 || R.n == 1024 || R.n == 2048 || R.n == 4096);
+}
+
 static bool dmux_fp_ok(const DevRing& R, const Gadget& g) {
   return R.ntt && R.nl == 2 && g.L == 2 && ntt_fp_ok(R.t[0], R.t[1]) && R.n == 2048;
 }
@@ -374,17 +443,16 @@ __global__ void k_cascade_reduce(const u64* __restrict__ P, int rank_in, int N, 
 //   bsum        =   sum_idx sum_s D[idx][s] K_idx[s].body
 // D: [lwe][idx][L][nl][n_in]; keys: [idx][L][2][nl][n_out]; mask_out:
 // [lwe][R/2][nl][n_out]. Block = TT slots x JJ output masks (TT * JJ = 256); the
-// JJ lanes' body partials are summed in shared memory. The body stays in the
-// eval domain through the cascade: body_out[lwe][l][t] = body_in[lwe][l][t/2] -
-// bsum (the eval form of embed_at(body_in, 0) - bsum, [lwe][nl][n_in] ->
-// [lwe][nl][n_out]). Small batches give few blocks: the output masks j are then
-// also split over JB blocks (blockIdx.x = slot block * JB + jb), and each block
-// writes its body partial to bpart[lwe][jb][nl][n_out] for k_cascade_bsum to add
-// up and apply.
+// JJ lanes' body partials are summed in shared memory. Small batches give few
+// blocks: the output masks j are then also split over JB blocks (blockIdx.x =
+// slot block * JB + jb). Every block adds its body partial (canonical, so at
+// most JB of them sum below 2^64) into this step's region of the zeroed
+// accumulator bsk: bsk[(lwe nl + l) * bsk_stride + t]. The body itself is only
+// needed after the last step (k_cascade_body_final).
 __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, const u64* __restrict__ keys, int R,
                                                      int n_in, int L, int TT, int JB, DevRing Rg,
-                                                     u64* __restrict__ mask_out, const u64* __restrict__ body_in,
-                                                     u64* __restrict__ body_out, u64* __restrict__ bpart) {
+                                                     u64* __restrict__ mask_out, u64* __restrict__ bsk,
+                                                     long bsk_stride) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
@@ -420,9 +488,10 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
     u64 acc = part[tl];
     for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
     if (JB == 1)
-      body_out[(lwe * nl + l) * n_out + t] = submod(body_in[(lwe * nl + l) * n_in + (t >> 1)], acc, m.q);
+      bsk[(lwe * nl + l) * bsk_stride + t] = acc;
     else
-      bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
+      atomicAdd(reinterpret_cast<unsigned long long*>(bsk + (lwe * nl + l) * bsk_stride + t),
+                (unsigned long long)acc);
   }
 }
 
@@ -434,8 +503,8 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
 // Two CTAs per SM leave room for nine digits' loads in flight per thread.
 __global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
                                                         int R, int n_in, int L, int TT, int JB, DevRing Rg,
-                                                        u64* __restrict__ mask_out, const u64* __restrict__ body_in,
-                                                        u64* __restrict__ body_out, u64* __restrict__ bpart) {
+                                                        u64* __restrict__ mask_out, u64* __restrict__ bsk,
+                                                        long bsk_stride) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
@@ -472,25 +541,31 @@ __global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restr
     u64 acc = part[tl];
     for (int x = 1; x < JJ; ++x) acc = addmod(acc, part[x * TT + tl], m.q);
     if (JB == 1)
-      body_out[(lwe * nl + l) * n_out + t] = submod(body_in[(lwe * nl + l) * n_in + (t >> 1)], acc, m.q);
+      bsk[(lwe * nl + l) * bsk_stride + t] = acc;
     else
-      bpart[((lwe * JB + jb) * nl + l) * n_out + t] = acc;
+      atomicAdd(reinterpret_cast<unsigned long long*>(bsk + (lwe * nl + l) * bsk_stride + t),
+                (unsigned long long)acc);
   }
 }
 
-// body_out[lwe][l][t] = body_in[lwe][l][t/2] - sum over jb of
-// bpart[lwe][jb][l][t] (mod q_l), all in the eval domain (k_cascade_mac).
-__global__ void k_cascade_bsum(const u64* __restrict__ bpart, int JB, int nl, int n_out, long nlwe, DevRing Rg,
-                               const u64* __restrict__ body_in, u64* __restrict__ body_out) {
+// The cascade's final body in the eval domain, [lwe][nl][n1] (n1 = 2^K). Step k
+// (output degree 2^(k+1)) maps body to embed_at(body, 0) - bsum_k, and the eval
+// form of embed_at repeats every slot, so
+//   body[t] = b - sum_k bsum_k[t >> (K - 1 - k)]
+// with b the LWE body (the degree-1 body, [lwe][nl]) and bsum_k the step's
+// accumulated sums, bsk[(lwe nl + l) * 2 n1 + 2^(k+1) - 2 + slot].
+__global__ void k_cascade_body_final(const u64* __restrict__ b0, const u64* __restrict__ bsk, int K, int nl,
+                                     long nlwe, DevRing Rg, u64* __restrict__ body) {
+  const int n1 = 1 << K;
   const long gid = (long)blockIdx.x * blockDim.x + threadIdx.x;
-  const long per = (long)nl * n_out;
-  if (gid >= nlwe * per) return;
-  const long lwe = gid / per, rem = gid % per;
-  const int l = (int)(rem / n_out), t = (int)(rem % n_out);
-  const u64 q = Rg.m[l].q;
+  if (gid >= nlwe * nl * n1) return;
+  const long ll = gid / n1;  // lwe * nl + l
+  const int t = (int)(gid % n1), l = (int)(ll % nl);
+  const DevMod& m = Rg.m[l];
+  const u64* sk = bsk + ll * 2 * n1;
   u64 acc = 0;
-  for (int jb = 0; jb < JB; ++jb) acc = addmod(acc, bpart[(lwe * JB + jb) * per + rem], q);
-  body_out[gid] = submod(body_in[(lwe * nl + l) * (n_out / 2) + (t >> 1)], acc, q);
+  for (int k = 0; k < K; ++k) acc = addmod(acc, reduce64(sk[(2 << k) - 2 + (t >> (K - 1 - k))], m), m.q);
+  body[gid] = submod(b0[ll], acc, m.q);
 }
 
 // body_out[lwe] = embed_at(body_in[lwe], N_out, 0) - bsum[lwe] (coefficient form).
@@ -611,7 +686,6 @@ struct Workspace {
   int bmax = 1;              // queries the buffers are sized for
   // Cascade.
   DevBuf c_masks_a, c_masks_b, c_body_a, c_body_b, c_digits, c_P, c_bsum, c_rlwe;
-  DevBuf c_bpart;  // k_cascade_mac body partials when the masks are split over blocks
   DevBuf c_dig8;   // 8-bit cascade / conversion-key digits [lwe][n1 * L_CK] bytes (base <= 255)
   // RLWE -> RGSW.
   // RGSWs grouped by use: the DMux bits of every query ([q][nd]), then the
@@ -693,11 +767,8 @@ static size_t workspace_build(Server& s, int bmax, Workspace* w, bool count_only
   // embedded degree); the other rings use the embedded digits and the P buffer.
   A(w->c_digits, nlwe * (s.r1.ntt ? 1 : 2) * n1 * Lck * nl);
   A(w->c_P, s.r1.ntt ? 0 : nlwe * 2 * n1 * 2 * nl);
-  A(w->c_bsum, nlwe * n1 * nl);
+  A(w->c_bsum, 2 * nlwe * n1 * nl);
   A(w->c_dig8, p.ck_base <= 255 && s.r1.ntt ? (nlwe * n1 * Lck + 7) / 8 : 0);
-  // A split grid has at most CASCADE_SPLIT_BLOCKS blocks of at most 256 slots.
-  // Two halves: the answer's stream and the side stream expand concurrently.
-  A(w->c_bpart, s.r1.ntt ? 2L * CASCADE_SPLIT_BLOCKS * 256 : 0);
   A(w->c_rlwe, nlwe * 2 * n1 * nl);
   A(w->g_digits, nlwe * Lck * nl * n1);
   A(w->g_gp, nlwe * 2 * nl * n1);
@@ -813,11 +884,10 @@ static void mod_switch(const DevRing& S, const u64* in, const DevRing& D, u64* o
 // Step 1: QueryDecomp (query_decomp.rs:39-95) of `nlwe` consecutive LWEs, the
 // first being LWE lwe0 of the workspace (LWE-indexed buffers are used from that
 // LWE's region on), forming the RGSWs of `nbits` query bits starting at bit
-// bit0 -> rgsw_q1 [bit][2L][2][nl][n1] (coefficient form). `bpart` is this
-// call's k_cascade_mac scratch. Disjoint (lwe0, nlwe) ranges may run
-// concurrently on different streams.
+// bit0 -> rgsw_q1 [bit][2L][2][nl][n1] (coefficient form). Disjoint (lwe0,
+// nlwe) ranges may run concurrently on different streams.
 static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long lwe0, long nlwe, long bit0,
-                               long nbits, u64* bpart, cudaStream_t st) {
+                               long nbits, cudaStream_t st) {
   const via_params& p = s.prm;
   const DevRing& R = s.r1;
   const int n1 = p.n1, nl = R.nl, L = p.l_ck;
@@ -828,11 +898,14 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
   u64* digits = w.c_digits.p + lwe0 * (R.ntt ? 1 : 2) * n1 * L * nl;
   u64* cP = R.ntt ? nullptr : w.c_P.p + lwe0 * 2 * n1 * 2 * nl;
   u64* bsum = w.c_bsum.p + lwe0 * lwe_n;
+  // Eval rings: every step's body sums, [lwe][nl][2 n1] (step regions of 2, 4, .. n1).
+  u64* bsk = w.c_bsum.p + lwe0 * 2 * lwe_n;
   u64* rlwe = w.c_rlwe.p + lwe0 * 2 * lwe_n;
   // Bases up to 255: digits as bytes, lifted and transformed by the 8-bit NTT.
   int8_t* dig8 = w.c_dig8.p ? reinterpret_cast<int8_t*>(w.c_dig8.p) + lwe0 * (long)n1 * L : nullptr;
   k_lwe_to_mlwe<<<blocks(nlwe * nl * (n1 + 1)), 256, 0, st>>>(d_query + lwe0 * (long)lwe_len(p), n1, nl, nlwe, mi, bi);
   VIA_LAUNCHED();
+  if (R.ntt) VIA_CUDA(cudaMemsetAsync(bsk, 0, (size_t)nlwe * 2 * lwe_n * 8, st));
   const u64 step_len = (u64)2 * n1 * L * 2 * nl;
   int k = 0;
   for (int n_in = 1; n_in < n1; n_in <<= 1, ++k) {
@@ -860,21 +933,19 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
       int JB = 1;
       while (JB * 2 <= iters && base * JB * 2 <= CASCADE_SPLIT_BLOCKS) JB *= 2;
       dim3 grid((unsigned)(n_out / tt * JB), (unsigned)nl, (unsigned)nlwe);
+      u64* bsk_k = bsk + (n_out - 2);  // this step's region
       if (fp_mac)
         k_cascade_mac_fp<<<grid, 256, 0, st>>>(reinterpret_cast<const double*>(digits),
                                                reinterpret_cast<const double*>(s.cascade_eval_d.p) + k * step_len,
-                                               rank_in, n_in, L, tt, JB, R, mo, bi, bo, bpart);
+                                               rank_in, n_in, L, tt, JB, R, mo, bsk_k, 2L * n1);
       else
         k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
-                                            bi, bo, bpart);
+                                            bsk_k, 2L * n1);
       VIA_LAUNCHED();
-      if (JB > 1) {
-        k_cascade_bsum<<<blocks(nlwe * nl * n_out), 256, 0, st>>>(bpart, JB, nl, n_out, nlwe, R, bi, bo);
-        VIA_LAUNCHED();
-      }
-      // The masks return to coefficient form for the next step's digits; the
-      // body stays in the eval domain until the last step.
+      // The masks return to coefficient form for the next step's digits.
       from_eval(R, mo, n_out, nlwe * (rank_in / 2) * nl, st);
+      std::swap(mi, mo);
+      continue;
     } else {
       gadget_product(R, w.g_ck, mi, n_out, 2, 1, polys, keys_cyclic(s.cascade_eval.p + k * step_len, rank_in), cP,
                      digits, st);
@@ -887,7 +958,12 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
     std::swap(mi, mo);
     std::swap(bi, bo);
   }
-  if (R.ntt) from_eval(R, bi, n1, nlwe * nl, st);  // the cascade's body, degree n1
+  if (R.ntt) {  // the cascade's body, from the LWE bodies in bi and every step's sums
+    k_cascade_body_final<<<blocks(nlwe * nl * n1), 256, 0, st>>>(bi, bsk, k, nl, nlwe, R, bo);
+    VIA_LAUNCHED();
+    from_eval(R, bo, n1, nlwe * nl, st);
+    std::swap(bi, bo);
+  }
   k_pack_rlwe<<<blocks(nlwe * nl * n1), 256, 0, st>>>(mi, bi, nlwe, n1, nl, rlwe);
   VIA_LAUNCHED();
   // RLWE -> RGSW with the conversion key (prim/gates/convert.rs:162-178); the
@@ -1423,15 +1499,14 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
   if (split) {
     VIA_CUDA(cudaEventRecord(w.ev_fork, st));
     VIA_CUDA(cudaStreamWaitEvent(w.side, w.ev_fork, 0));
-    query_decomp_range(s, w, qsrc, B * lwe_a, nlwe_all - B * lwe_a, B * nd, B * nb,
-                       w.c_bpart.p + CASCADE_SPLIT_BLOCKS * 256, w.side);
+    query_decomp_range(s, w, qsrc, B * lwe_a, nlwe_all - B * lwe_a, B * nd, B * nb, w.side);
     mod_switch(s.r1, rgsw_b1, s.r2, rgsw_b2, B * nb * 2 * L * 2, n1, w.side);
     to_eval(s.r2, rgsw_b2, n1, B * nb * 2 * L * 2, w.side);
     VIA_CUDA(cudaEventRecord(w.ev_join, w.side));
-    query_decomp_range(s, w, qsrc, 0, B * lwe_a, 0, B * nd, w.c_bpart.p, st);
+    query_decomp_range(s, w, qsrc, 0, B * lwe_a, 0, B * nd, st);
     to_eval(s.r1, w.rgsw_q1.p, n1, B * nd * 2 * L * 2 * nl, st);
   } else {
-    query_decomp_range(s, w, qsrc, 0, nlwe_all, 0, B * w.nbits, w.c_bpart.p, st);
+    query_decomp_range(s, w, qsrc, 0, nlwe_all, 0, B * w.nbits, st);
     if (stop_stage == 1) return copy_out(w.c_rlwe.p, (size_t)w.nlwe * 2 * nl * n1);
     if (stop_stage == 2) return copy_out(w.rgsw_q1.p, (size_t)w.nbits * rgsw1);  // one query: bit order
 
@@ -1459,6 +1534,12 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
       if (dmux_fp_ok(s.r1, w.g_dmux) && B * active >= 256) {
         k_dmux_fp<11><<<dim3((unsigned)(B * active), 2), 256, 0, st>>>(out, in, bit, s.r1, w.g_dmux);
         VIA_LAUNCHED();
+        std::swap(in, out);
+        continue;
+      }
+      if (R_fp_small(s.r1)) {
+        external_products(s.r1, w.g_dmux, bit, in, B * active, w.dm_digits.p, w.dm_ext.p, false, st);
+        intt_epi<INTT_DMUX>(s.r1, w.dm_ext.p, in, out, B * active, st);
         std::swap(in, out);
         continue;
       }
@@ -1507,8 +1588,10 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
     cur = nxt;
   }
   // Selected columns back to coefficient form.
-  VIA_CUDA(cudaMemcpyAsync(w.cr_ct.p, cur, (size_t)B * 2 * n1 * 8, cudaMemcpyDeviceToDevice, st));
-  from_eval(s.r2, w.cr_ct.p, n1, B * 2, st);
+  if (!intt_epi<INTT_STORE>(s.r2, cur, nullptr, w.cr_ct.p, B, st)) {
+    VIA_CUDA(cudaMemcpyAsync(w.cr_ct.p, cur, (size_t)B * 2 * n1 * 8, cudaMemcpyDeviceToDevice, st));
+    from_eval(s.r2, w.cr_ct.p, n1, B * 2, st);
+  }
   if (stop_stage == 6) return copy_out(w.cr_ct.p, 2 * (size_t)n1);
 
   // ---- Step 6: CRot, SlotExtract (rotate.rs:128-150).
@@ -1516,6 +1599,11 @@ void answer_device_stages(Server& s, Workspace& w, const u64* d_query, int nq, u
     k_crot_diff_batch<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, n1, n1 - (1 << i), B, s.r2.m[0], w.cr_diff.p);
     VIA_LAUNCHED();
     KeySel bit{rgsw_b2 + (nc + i) * rgsw2, 1, B, nb * rgsw2};
+    if (R_fp_small(s.r2)) {
+      external_products(s.r2, w.g_cmux, bit, w.cr_diff.p, B, w.cr_digits.p, w.cr_ext.p, false, st);
+      intt_epi<INTT_ADD>(s.r2, w.cr_ext.p, w.cr_ct.p, w.cr_ct.p, B, st);
+      continue;
+    }
     external_products(s.r2, w.g_cmux, bit, w.cr_diff.p, B, w.cr_digits.p, w.cr_ext.p, true, st);
     k_rlwe_addsub<<<blocks(B * 2 * n1), 256, 0, st>>>(w.cr_ct.p, w.cr_ct.p, 1, w.cr_ext.p, 1, +1, B, n1, 1, s.r2);
     VIA_LAUNCHED();
