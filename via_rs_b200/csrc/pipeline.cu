@@ -501,10 +501,13 @@ __global__ void __launch_bounds__(256) k_cascade_mac(const u64* __restrict__ D, 
 // so a mask's 2 L products stay below 1.125 L q; the body partial is brought
 // back within q/2 after each output mask's 2 L products. Outputs as k_cascade_mac.
 // Two CTAs per SM leave room for nine digits' loads in flight per thread.
-__global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restrict__ D, const double* __restrict__ keys,
-                                                        int R, int n_in, int L, int TT, int JB, DevRing Rg,
-                                                        u64* __restrict__ mask_out, u64* __restrict__ bsk,
-                                                        long bsk_stride) {
+// I8 (the first step, n_in = 1): the digits are read as the signed bytes of
+// k_decompose_i8, [lwe][idx][L], whose transform at degree 1 is the digit itself.
+template <bool I8>
+__global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restrict__ D, const int8_t* __restrict__ D8,
+                                                        const double* __restrict__ keys, int R, int n_in, int L,
+                                                        int TT, int JB, DevRing Rg, u64* __restrict__ mask_out,
+                                                        u64* __restrict__ bsk, long bsk_stride) {
   __shared__ u64 part[256];
   const int nl = Rg.nl, n_out = 2 * n_in, half = R / 2;
   const int JJ = 256 / TT;
@@ -525,9 +528,11 @@ __global__ void __launch_bounds__(256, 2) k_cascade_mac_fp(const double* __restr
     const double* d1 = Dw + (long)(j + half) * L * dper;
     const double* k0 = Kl + (long)j * L * 2 * kper;
     const double* k1 = Kl + (long)(j + half) * L * 2 * kper;
+    const int8_t* e0 = D8 + (lwe * R + j) * L;
+    const int8_t* e1 = D8 + (lwe * R + j + half) * L;
 #pragma unroll 9
     for (int s = 0; s < L; ++s) {
-      const double a = d0[s * dper], b = d1[s * dper];
+      const double a = I8 ? (double)e0[s] : d0[s * dper], b = I8 ? (double)e1[s] : d1[s * dper];
       am = __dadd_rn(am, __dadd_rn(fp_mulmod(a, k0[(2 * s) * kper], q, qinv), fp_mulmod(b, k1[(2 * s) * kper], q, qinv)));
       ab = __dadd_rn(ab, __dadd_rn(fp_mulmod(a, k0[(2 * s + 1) * kper], q, qinv),
                                    fp_mulmod(b, k1[(2 * s + 1) * kper], q, qinv)));
@@ -913,11 +918,13 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
     const long polys = nlwe * rank_in;
     if (R.ntt) {
       // Digits at the input degree; see k_cascade_mac for the repeated slots.
-      const bool fp_mac = dig8 && n_in > 1 && s.cascade_eval_d.p;
-      if (dig8 && n_in > 1) {
+      const bool fp_mac = dig8 && s.cascade_eval_d.p;
+      if (dig8 && (n_in > 1 || fp_mac)) {
         k_decompose_i8<<<blocks(polys * n_in, 128), 128, 0, st>>>(mi, n_in, polys, R, w.g_ck, dig8);
         VIA_LAUNCHED();
-        if (fp_mac)
+        if (n_in == 1)
+          ;  // degree 1: the MAC reads the digits themselves
+        else if (fp_mac)
           ntt_forward_i8_fp(dig8, reinterpret_cast<double*>(digits), n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
         else
           ntt_forward_i8_lazy(dig8, digits, n_in, nl, polys * L * nl, R.t[0], R.t[1], st);
@@ -934,10 +941,12 @@ static void query_decomp_range(Server& s, Workspace& w, const u64* d_query, long
       while (JB * 2 <= iters && base * JB * 2 <= CASCADE_SPLIT_BLOCKS) JB *= 2;
       dim3 grid((unsigned)(n_out / tt * JB), (unsigned)nl, (unsigned)nlwe);
       u64* bsk_k = bsk + (n_out - 2);  // this step's region
-      if (fp_mac)
-        k_cascade_mac_fp<<<grid, 256, 0, st>>>(reinterpret_cast<const double*>(digits),
-                                               reinterpret_cast<const double*>(s.cascade_eval_d.p) + k * step_len,
-                                               rank_in, n_in, L, tt, JB, R, mo, bsk_k, 2L * n1);
+      const double* kd = reinterpret_cast<const double*>(s.cascade_eval_d.p) + k * step_len;
+      if (fp_mac && n_in == 1)
+        k_cascade_mac_fp<true><<<grid, 256, 0, st>>>(nullptr, dig8, kd, rank_in, n_in, L, tt, JB, R, mo, bsk_k, 2L * n1);
+      else if (fp_mac)
+        k_cascade_mac_fp<false><<<grid, 256, 0, st>>>(reinterpret_cast<const double*>(digits), dig8, kd, rank_in, n_in,
+                                                      L, tt, JB, R, mo, bsk_k, 2L * n1);
       else
         k_cascade_mac<<<grid, 256, 0, st>>>(digits, s.cascade_eval.p + k * step_len, rank_in, n_in, L, tt, JB, R, mo,
                                             bsk_k, 2L * n1);
