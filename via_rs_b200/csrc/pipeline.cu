@@ -1013,106 +1013,10 @@ static void external_products(const DevRing& R, const Gadget& g, KeySel rgsw, co
 //   RGSW samples (mask digits with neg_s_m, body digits with m, digit k with
 //   sample L-1-k) -> out[o] = in[2o] + ext, eval form throughout.
 // cur: [count*2][2][n]; nxt: [count][2][n]; the RGSW of CMux o ([2L][2][n],
-// eval) is picked by `ks`. The digits never leave registers.
-// Sum of products of residues below 2^40: each product's high word is below
-// 2^16, so up to 2^16 products fit a 32-bit high word. The digit transforms'
-// lazy outputs stay below (1 + 2 LOGN) q < 2^40 for q < 2^35 (cmux_fused_ok).
-// Three registers instead of four.
-struct Acc96 {
-  u64 lo;
-  u32 hi;
-};
-__device__ __forceinline__ void mac96(Acc96& acc, u64 a, u64 b) {
-  const u64 pl = a * b;
-  const u32 ph = (u32)mulhi(a, b);
-  const u64 nl = acc.lo + pl;
-  acc.hi += ph + (nl < pl ? 1u : 0u);
-  acc.lo = nl;
-}
-
-template <int LOGN>
-__global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fused(const u64* __restrict__ cur, u64* __restrict__ nxt,
-                                                                  KeySel ks, DevRing R, Gadget g) {
-  constexpr int n = 1 << LOGN;
-  using In0 = NttPhase<LOGN, true, 0>;
-  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
-  using Fw0 = NttPhase<LOGN, false, 0>;
-  using FwL = NttPhase<LOGN, false, (LOGN + 2) / 3 - 1>;
-  // The inverse's input and the forward's output layouts are 8 consecutive
-  // residues per thread (slot 8 tid + v), so those accesses are 16-byte vectors.
-  static_assert(In0::STRIDE == 1 && In0::R == 3 && FwL::STRIDE == 1, "contiguous end layouts");
-  __shared__ u64 ssm[n];
-  const int tid = threadIdx.x;
-  const long o = blockIdx.x;
-  const NttTable& T = R.t[0];
-  const DevMod& m = R.m[0];
-  const u64 q = m.q;
-  const u64* a = cur + (2 * o) * 2 * n;
-  const u64* b = a + 2 * n;
-  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
-  const int L = g.L;
-  Acc96 am[8], ab[8];
-#pragma unroll
-  for (int v = 0; v < 8; ++v) am[v] = ab[v] = Acc96{0, 0};
-  for (int p = 0; p < 2; ++p) {  // 0: mask digits (neg_s_m rows), 1: body digits (m rows)
-    u64 e[8];
-    {
-      const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
-      const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const ulonglong2 x = bv[h], y = av[h];
-        e[2 * h] = submod(x.x, y.x, q);
-        e[2 * h + 1] = submod(x.y, y.y, q);
-      }
-    }
-    ntt_inverse_regs<LOGN>(e, tid, T, ssm);
-    __syncthreads();
-#pragma unroll
-    for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
-    __syncthreads();
-    u32 dcur[8];  // scaled coefficients, below B^L < 2^32
-#pragma unroll
-    for (int v = 0; v < 8; ++v) dcur[v] = (u32)gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
-    for (int k = 0; k < L; ++k) {
-#pragma unroll
-      for (int v = 0; v < 8; ++v) e[v] = lift_i64(gadget_next_digit32(dcur[v], g), m);
-      // Lazy outputs (below (1 + 2 LOGN) q < 2^40 for q < 2^35) feed the 96-bit sums directly.
-      ntt_forward_regs<LOGN, 0, true>(e, tid, T, ssm);
-      const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * (p * L + L - 1 - k)) * n + 8 * tid);
-      const ulonglong2* Kb = Km + n / 2;
-#pragma unroll
-      for (int h = 0; h < 4; ++h) {
-        const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
-        mac96(am[2 * h], e[2 * h], km.x);
-        mac96(am[2 * h + 1], e[2 * h + 1], km.y);
-        mac96(ab[2 * h], e[2 * h], kb.x);
-        mac96(ab[2 * h + 1], e[2 * h + 1], kb.y);
-      }
-    }
-  }
-  ulonglong2* outm = reinterpret_cast<ulonglong2*>(nxt + o * 2 * n + 8 * tid);
-  ulonglong2* outb = outm + n / 2;
-  const ulonglong2* am_in = reinterpret_cast<const ulonglong2*>(a + 8 * tid);
-  const ulonglong2* ab_in = am_in + n / 2;
-#pragma unroll
-  for (int h = 0; h < 4; ++h) {
-    const ulonglong2 xm = am_in[h], xb = ab_in[h];
-    ulonglong2 ym, yb;
-    ym.x = addmod(xm.x, reduce128(am[2 * h].hi, am[2 * h].lo, m), q);
-    ym.y = addmod(xm.y, reduce128(am[2 * h + 1].hi, am[2 * h + 1].lo, m), q);
-    yb.x = addmod(xb.x, reduce128(ab[2 * h].hi, ab[2 * h].lo, m), q);
-    yb.y = addmod(xb.y, reduce128(ab[2 * h + 1].hi, ab[2 * h + 1].lo, m), q);
-    outm[h] = ym;
-    outb[h] = yb;
-  }
-}
-
-// k_cmux_fused in double precision (ntt_fp.cuh): the same CMux per CTA, the
-// same layouts and digits, with every transform and RGSW product computed as
-// exact integer arithmetic on doubles (FMA two-products and a floating-point
-// quotient estimate) instead of emulated 64-bit integer products. For single
-// primes q < 2^35 and small gadgets: differences of canonical residues are
+// eval) is picked by `ks`. The digits never leave registers. Every transform
+// and RGSW product is exact integer arithmetic on doubles (ntt_fp.cuh: FMA
+// two-products and a floating-point quotient estimate). For single primes
+// q < 2^35 and small gadgets: differences of canonical residues are
 // below q; the inverse leaves coefficients within 0.5625 q, made canonical for
 // the digit split; digits below B/2 transform to values below 7 q; each product
 // with an RGSW sample (below q) is reduced to within 0.5625 q, so the 2L
@@ -1197,7 +1101,7 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fp
   }
 }
 
-// The CMux of k_cmux_fused split over a cluster of four CTAs, for tree levels
+// The CMux of k_cmux_fp split over a cluster of four CTAs, for tree levels
 // with too few CMuxes to fill the GPU, where one CMux's latency sets the level's
 // time. CTA r of the cluster takes input half p = r & 1 (mask or body),
 // inverse-transforms its difference, and forward-transforms its digit k = r >> 1;
@@ -1207,83 +1111,9 @@ __global__ void __launch_bounds__((1 << LOGN) / 8, LOGN >= 12 ? 1 : 2) k_cmux_fp
 // memory; a second barrier keeps every CTA's shared memory alive until those
 // reads are done. Two transforms per CTA instead of six for one CTA. L = 2 and
 // n <= 2048 (48 KB of static shared memory).
-template <int LOGN>
-__global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
-    k_cmux_cluster(const u64* __restrict__ cur, u64* __restrict__ nxt, KeySel ks, DevRing R, Gadget g) {
-  namespace cg = cooperative_groups;
-  constexpr int n = 1 << LOGN;
-  using InL = NttPhase<LOGN, true, (LOGN + 2) / 3 - 1>;
-  using Fw0 = NttPhase<LOGN, false, 0>;
-  __shared__ u64 ssm[n];    // transform exchanges, then the mask partial
-  __shared__ u64 pbody[n];  // the body partial
-  cg::cluster_group cluster = cg::this_cluster();
-  const int r = (int)cluster.block_rank();
-  const int p = r & 1, k = r >> 1;
-  const int tid = threadIdx.x;
-  const long o = blockIdx.x / 4;
-  const NttTable& T = R.t[0];
-  const DevMod& m = R.m[0];
-  const u64 q = m.q;
-  const u64* a = cur + (2 * o) * 2 * n;
-  const u64* b = a + 2 * n;
-  const u64* K = ks.base + ((o / ks.div) % ks.mod) * ks.stride;
-  u64 e[8];
-  {
-    const ulonglong2* bv = reinterpret_cast<const ulonglong2*>(b + p * n + 8 * tid);
-    const ulonglong2* av = reinterpret_cast<const ulonglong2*>(a + p * n + 8 * tid);
-#pragma unroll
-    for (int h = 0; h < 4; ++h) {
-      const ulonglong2 x = bv[h], y = av[h];
-      e[2 * h] = submod(x.x, y.x, q);
-      e[2 * h + 1] = submod(x.y, y.y, q);
-    }
-  }
-  ntt_inverse_regs<LOGN>(e, tid, T, ssm);
-  __syncthreads();
-#pragma unroll
-  for (int v = 0; v < 8; ++v) ssm[swz(InL::index(v, tid))] = e[v];
-  __syncthreads();
-#pragma unroll
-  for (int v = 0; v < 8; ++v) {
-    u32 c = (u32)gadget_scaled_small(ssm[swz(Fw0::index(v, tid))], g);
-    i64 d = gadget_next_digit32(c, g);
-    if (k) d = gadget_next_digit32(c, g);
-    e[v] = lift_i64(d, m);
-  }
-  ntt_forward_regs<LOGN>(e, tid, T, ssm);
-  const int smp = p * 2 + 1 - k;  // sample L - 1 - k of half p (L = 2)
-  const ulonglong2* Km = reinterpret_cast<const ulonglong2*>(K + (long)(2 * smp) * n + 8 * tid);
-  const ulonglong2* Kb = Km + n / 2;
-  __syncthreads();  // every thread is done with the transform's exchanges in ssm
-#pragma unroll
-  for (int h = 0; h < 4; ++h) {
-    const ulonglong2 km = __ldg(Km + h), kb = __ldg(Kb + h);
-    const int s0 = 8 * tid + 2 * h;
-    ssm[s0] = reduce128(mulhi(e[2 * h], km.x), e[2 * h] * km.x, m);
-    ssm[s0 + 1] = reduce128(mulhi(e[2 * h + 1], km.y), e[2 * h + 1] * km.y, m);
-    pbody[s0] = reduce128(mulhi(e[2 * h], kb.x), e[2 * h] * kb.x, m);
-    pbody[s0 + 1] = reduce128(mulhi(e[2 * h + 1], kb.y), e[2 * h + 1] * kb.y, m);
-  }
-  cluster.sync();
-  if (r < 2) {  // rank 0: the output mask, rank 1: the output body
-    u64* parts[4];
-#pragma unroll
-    for (int rr = 0; rr < 4; ++rr) parts[rr] = cluster.map_shared_rank(r == 0 ? ssm : pbody, rr);
-    u64* out = nxt + o * 2 * n + (long)r * n;
-    for (int x = tid; x < n; x += blockDim.x) {
-      u64 acc = a[(long)r * n + x];
-#pragma unroll
-      for (int rr = 0; rr < 4; ++rr) acc = addmod(acc, parts[rr][x], q);
-      out[x] = acc;
-    }
-  }
-  cluster.sync();
-}
-
-// k_cmux_cluster in double precision (ntt_fp.cuh), with the bounds of
-// k_cmux_fp: each CTA's products are signed residues within 0.5625 q, kept as
-// doubles in shared memory; ranks 0 and 1 add the four partials to in[2o] and
-// reduce once.
+// In double precision with the bounds of k_cmux_fp: each CTA's products are
+// signed residues within 0.5625 q, kept as doubles in shared memory; ranks 0
+// and 1 add the four partials to in[2o] and reduce once.
 template <int LOGN>
 __global__ void __cluster_dims__(4, 1, 1) __launch_bounds__((1 << LOGN) / 8, 2)
     k_cmux_cluster_fp(const u64* __restrict__ cur, u64* __restrict__ nxt, KeySel ks, DevRing R, Gadget g) {
