@@ -214,7 +214,8 @@ via_status via_first_dim_scan_many_dev(via_server* s, const uint64_t* sel_eval, 
  * CTAs walk the (slot, column-tile) units in. Every tile gives the same exact
  * result. via_server_autotune times every candidate tile for each listed batch
  * size on this server's database (CUDA events, one warm-up and three timed
- * scans each) and keeps the fastest; scans of other batch sizes use the entry
+ * scans each, in two passes over the candidates) and keeps the candidate whose
+ * faster pass is fastest; scans of other batch sizes use the entry
  * of the nearest tuned size above (else below) of the same kind (one query, or
  * a batch). With a cache_path, entries measured before for the same device,
  * ring degree, grid and modulus are read from that file instead of measured,
